@@ -1,0 +1,1521 @@
+// bls_engine.cu -- B200 (sm_100a) Box Least Squares engine behind the C ABI of
+// include/astrotransit_b200.h.
+//
+// Hot path (one astropy-style BLS per (light curve, period)):
+//   stage kernel   one CTA per curve: t_start = t[0], dt = t - t_start (FP64),
+//                  deterministic fixed-point staging q_w = rint(w*2^s_w),
+//                  q_y = rint(w*(y-c)*2^s_y) (|q| <= 2^26), per-curve totals.
+//   search kernel  persistent; CTAs pop (curve, 64-period) tiles from a device
+//                  counter.  Periods of a tile are packed into groups whose
+//                  histograms fit shared memory; each thread keeps 8
+//                  consecutive points in registers and folds them into every
+//                  period of the group (FP64 fold, identical to the reference's
+//                  per-point formula), merging runs of equal bins in registers
+//                  before a 64-bit shared-memory reduction.  Teams of warps
+//                  then scan each histogram (exact int64 -> exact FP64),
+//                  evaluate every (start, duration) window in FP32 with an
+//                  exact rational comparison, and re-evaluate the winner in
+//                  FP64.
+//   best kernel    per-curve argmax over the period grid.
+//
+// Reference semantics followed (paths within ubunbun18/Astro_Transit_GPU):
+//   astropy-binned geometry  search/kernels/vbls_v42_parity.cu:36-129
+//   fixed-bin geometry       search/kernels/bls.cu:47-169
+//   host prologues           search/v42_parity.py:42-67, search/gpu_bls.py:57-78
+//
+// Build: nvcc -gencode arch=compute_100a,code=sm_100a -fmad=false (every
+// intended fused multiply-add is an explicit fma()), see build.py.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/astrotransit_b200.h"
+
+#define ATB_VERSION "astrotransit-b200 0.1.0 sm_100a"
+
+namespace {
+
+constexpr int kBlock = 512;            // threads of a search CTA
+constexpr int kWarps = kBlock / 32;    // 16
+constexpr int kR = 8;                  // consecutive points a thread holds in registers
+constexpr int kTileP = 64;             // periods per work-queue tile
+constexpr int kMaxG = 64;              // periods per shared-memory group
+constexpr int kMaxDur = 32;            // durations per curve
+constexpr int kQBits = 26;             // |q| <= 2^kQBits per point
+constexpr int kStageAlign = 32;        // staged curves start at multiples of 32 points
+constexpr int kStageBlock = 256;
+
+struct CurveStat {
+    double t_start;
+    double shift;
+    long long qw_tot;
+    long long qy_tot;
+    long long qy_abs;
+    int s_w;
+    int s_y;
+    double bin_dur;      // BINNED: min(duration) / oversample
+    double inv_bin_dur;  // BINNED: 1 / bin_dur
+    int n_dur;
+    int pad;
+};
+
+struct StageArgs {
+    const long long* pt_off;
+    const long long* t_off;
+    const long long* stage_off;
+    const long long* dur_beg;
+    const int* dur_cnt;
+    const double* t;
+    const void* y;
+    const float* w;
+    const double* durations;
+    double* sdt;
+    int* sqw;
+    int* sqy;
+    CurveStat* stats;
+    int* dbins;  // [n_curves * kMaxDur]
+    int oversample;
+    int* status;
+};
+
+struct SearchArgs {
+    int objective;
+    int n_bins_fixed;
+    int oversample;
+    int max_bins;
+    int n_curves;
+    int cap;  // shared-memory histogram entries
+    long long n_tiles;
+    const long long* pt_off;
+    const long long* stage_off;
+    const long long* per_beg;
+    const long long* per_cnt;
+    const long long* dur_beg;
+    const int* dur_cnt;
+    const long long* out_beg;
+    const long long* tile_off;
+    const int* order;
+    const double* periods;
+    const double* durations;
+    const double* sdt;
+    const int* sqw;
+    const int* sqy;
+    const CurveStat* stats;
+    const int* dbins;
+    float* power;
+    float* depth;
+    float* depth_err;
+    double* t0;
+    float* duration;
+    int* window;
+    longlong2* ghist;
+    long long ghist_stride;
+    unsigned long long* tile_counter;
+    int* status;
+};
+
+// ----------------------------------------------------------------------------
+// shared device helpers
+// ----------------------------------------------------------------------------
+
+__device__ __forceinline__ int q_scale(double m) {
+    if (!(m > 0.0)) return 0;
+    int e;
+    frexp(m, &e);
+    return kQBits - e;
+}
+
+__device__ __forceinline__ double ll_as_d(long long v) { return __longlong_as_double(v); }
+
+// V42 bin count, vbls_v42_parity.cu:46-47 (cap only when max_bins > 0)
+__device__ __forceinline__ int binned_nbins(double period, double inv_bin_dur, int oversample,
+                                            int max_bins) {
+    double x = ceil(period * inv_bin_dur);
+    if (!(x < 1.0e9)) x = 1.0e9;
+    int nb = (int)x + oversample;
+    if (max_bins > 0 && nb >= max_bins) nb = max_bins - 1;
+    return nb;
+}
+
+// astropy-binned fold: ph = t - P*floor(t/P) (fused), ind = int(ph/bin_dur)+1
+// (vbls_v42_parity.cu:65-70); returns the histogram slot in [0, nb].
+__device__ __forceinline__ int fold_binned(double d, double period, double inv_period,
+                                           double inv_bin_dur, int nb) {
+    const double m = d * inv_period;
+    const double ph = fma(-period, floor(m), d);
+    const double x = ph * inv_bin_dur;
+    int ind = __double2int_rz(x) + 1;
+    ind = min(ind, nb);
+    ind = max(ind, 0);
+    return ind;
+}
+
+// fixed-bin fold: phase = frac(t_rel*inv_p), bin = int(phase*n_bins) (bls.cu:52-62);
+// returns bin+1, or the trash slot nb+1 for points the reference drops.
+__device__ __forceinline__ int fold_fixed(double d, double inv_p, double nbd, int nb) {
+    const double m = d * inv_p;
+    const double ph = m - floor(m);
+    const int b = __double2int_rz(ph * nbd);
+    return (b >= 0 && b < nb) ? b + 1 : nb + 1;
+}
+
+// Exact comparison of candidates a = an/ad and b = bn/bd (floats, positive
+// denominators): products split into rounded value + exact fma residual.
+// Equal ratios are ordered by the smaller window key.
+__device__ __forceinline__ bool cand_better(float an, float ad, int ak, float bn, float bd,
+                                            int bk) {
+    const float p = __fmul_rn(an, bd);
+    const float q = __fmul_rn(bn, ad);
+    if (p != q) return p > q;
+    const float e1 = __fmaf_rn(an, bd, -p);
+    const float e2 = __fmaf_rn(bn, ad, -q);
+    if (e1 != e2) return e1 > e2;
+    return ak < bk;
+}
+
+struct Cand {
+    float num, den;
+    int key;
+};
+
+__device__ __forceinline__ void cand_consider(Cand& b, float num, float den, int key) {
+    if (cand_better(num, den, key, b.num, b.den, b.key)) {
+        b.num = num;
+        b.den = den;
+        b.key = key;
+    }
+}
+
+__device__ __forceinline__ Cand warp_best(Cand c) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const float on = __shfl_down_sync(0xffffffffu, c.num, off);
+        const float od = __shfl_down_sync(0xffffffffu, c.den, off);
+        const int ok = __shfl_down_sync(0xffffffffu, c.key, off);
+        if (cand_better(on, od, ok, c.num, c.den, c.key)) {
+            c.num = on;
+            c.den = od;
+            c.key = ok;
+        }
+    }
+    return c;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_max(T v) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, off));
+    return v;
+}
+
+__device__ __forceinline__ long long warp_sum(long long v) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    return v;
+}
+
+// block reductions for the stage kernel (kStageBlock threads)
+__device__ double block_max_d(double v, double* sh) {
+    v = warp_max(v);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    double r = sh[0];
+    for (int i = 1; i < kStageBlock / 32; ++i) r = max(r, sh[i]);
+    return r;
+}
+
+__device__ long long block_sum_ll(long long v, long long* sh) {
+    v = warp_sum(v);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    long long r = 0;
+    for (int i = 0; i < kStageBlock / 32; ++i) r += sh[i];
+    return r;
+}
+
+// ----------------------------------------------------------------------------
+// stage kernel: one CTA per light curve
+// ----------------------------------------------------------------------------
+
+template <typename YT>
+__global__ void __launch_bounds__(kStageBlock) stage_kernel(const StageArgs a) {
+    __shared__ double shd[kStageBlock / 32];
+    __shared__ long long shl[kStageBlock / 32];
+    const int c = blockIdx.x;
+    const long long p0 = a.pt_off[c];
+    const long long n = a.pt_off[c + 1] - p0;
+    const long long tb = a.t_off ? a.t_off[c] : p0;
+    const double* t = a.t + tb;
+    const YT* y = static_cast<const YT*>(a.y) + p0;
+    const float* w = a.w ? a.w + p0 : nullptr;
+    const long long so = a.stage_off[c];
+    const long long n_pad = (n + kR - 1) / kR * kR;
+
+    // pass 1: magnitudes and validity
+    double wmax = 0.0, amax = 0.0;
+    int bad = 0;
+    for (long long i = threadIdx.x; i < n; i += kStageBlock) {
+        const double wi = w ? (double)w[i] : 1.0;
+        const double yi = (double)y[i];
+        if (!(wi > 0.0) || !isfinite(wi) || !isfinite(yi) || !isfinite(t[i])) bad = 1;
+        wmax = max(wmax, wi);
+        amax = max(amax, fabs(wi * yi));
+    }
+    wmax = block_max_d(wmax, shd);
+    amax = block_max_d(amax, shd);
+    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(a.status, 1);
+    const int s_w = q_scale(wmax);
+    const int s_a = q_scale(amax);
+
+    // pass 2: exact integer sums -> the shift c (weighted mean of y)
+    long long sqw = 0, sqa = 0;
+    for (long long i = threadIdx.x; i < n; i += kStageBlock) {
+        const double wi = w ? (double)w[i] : 1.0;
+        const double yi = (double)y[i];
+        sqw += __double2ll_rn(ldexp(wi, s_w));
+        sqa += __double2ll_rn(ldexp(wi * yi, s_a));
+    }
+    sqw = block_sum_ll(sqw, shl);
+    sqa = block_sum_ll(sqa, shl);
+    const double shift = sqw != 0 ? ldexp((double)sqa / (double)sqw, s_w - s_a) : 0.0;
+
+    // pass 3: magnitude of w*(y - c)
+    double vmax = 0.0;
+    for (long long i = threadIdx.x; i < n; i += kStageBlock) {
+        const double wi = w ? (double)w[i] : 1.0;
+        vmax = max(vmax, fabs(wi * ((double)y[i] - shift)));
+    }
+    vmax = block_max_d(vmax, shd);
+    const int s_y = q_scale(vmax);
+
+    // pass 4: staged arrays (padded with zero-weight points) and totals
+    const double t_start = n > 0 ? t[0] : 0.0;
+    long long qw_tot = 0, qy_tot = 0, qy_abs = 0;
+    for (long long i = threadIdx.x; i < n_pad; i += kStageBlock) {
+        double d = 0.0;
+        int qa = 0, qb = 0;
+        if (i < n) {
+            const double wi = w ? (double)w[i] : 1.0;
+            qa = (int)__double2ll_rn(ldexp(wi, s_w));
+            qb = (int)__double2ll_rn(ldexp(wi * ((double)y[i] - shift), s_y));
+            d = t[i] - t_start;
+        }
+        a.sdt[so + i] = d;
+        a.sqw[so + i] = qa;
+        a.sqy[so + i] = qb;
+        qw_tot += qa;
+        qy_tot += qb;
+        qy_abs += qb < 0 ? -(long long)qb : (long long)qb;
+    }
+    qw_tot = block_sum_ll(qw_tot, shl);
+    qy_tot = block_sum_ll(qy_tot, shl);
+    qy_abs = block_sum_ll(qy_abs, shl);
+
+    if (threadIdx.x == 0) {
+        const int nd = a.dur_cnt[c];
+        const double* dur = a.durations + a.dur_beg[c];
+        double min_dur = dur[0];
+        for (int k = 1; k < nd; ++k) min_dur = min(min_dur, dur[k]);
+        if (!(min_dur > 0.0) || !isfinite(min_dur)) atomicOr(a.status, 2);
+        const double bin_dur = min_dur / (double)a.oversample;
+        const double ibd = 1.0 / bin_dur;
+        for (int k = 0; k < nd; ++k) a.dbins[c * kMaxDur + k] = (int)round(dur[k] * ibd);
+        CurveStat st;
+        st.t_start = t_start;
+        st.shift = shift;
+        st.qw_tot = qw_tot;
+        st.qy_tot = qy_tot;
+        st.qy_abs = qy_abs;
+        st.s_w = s_w;
+        st.s_y = s_y;
+        st.bin_dur = bin_dur;
+        st.inv_bin_dur = ibd;
+        st.n_dur = nd;
+        st.pad = 0;
+        a.stats[c] = st;
+    }
+}
+
+// ----------------------------------------------------------------------------
+// search kernel
+// ----------------------------------------------------------------------------
+
+template <bool GLOB>
+__device__ __forceinline__ void hist_add(longlong2* H, int slot, int aw, int ay) {
+    if (GLOB) {
+        atomicAdd(reinterpret_cast<unsigned long long*>(&H[slot].x),
+                  (unsigned long long)(long long)aw);
+        atomicAdd(reinterpret_cast<unsigned long long*>(&H[slot].y),
+                  (unsigned long long)(long long)ay);
+    } else {
+        const unsigned addr = (unsigned)__cvta_generic_to_shared(&H[slot]);
+        asm volatile("red.shared.add.u64 [%0], %1;" ::"r"(addr), "l"((long long)aw) : "memory");
+        asm volatile("red.shared.add.u64 [%0+8], %1;" ::"r"(addr), "l"((long long)ay) : "memory");
+    }
+}
+
+struct Team {
+    int id;        // team index
+    int nthreads;  // 32 * warps
+    int nwarps;
+    int tid;       // thread index within the team
+    int warp0;     // first block-level warp of the team
+};
+
+__device__ __forceinline__ void team_sync(const Team& tm) {
+    if (tm.nwarps == 1) {
+        __syncwarp();
+    } else {
+        asm volatile("bar.sync %0, %1;" ::"r"(tm.id + 1), "r"(tm.nthreads) : "memory");
+    }
+}
+
+struct GroupSmem {
+    double P[kMaxG];
+    double IP[kMaxG];
+    int NB[kMaxG];
+    int base[kMaxG];
+    long long slot[kMaxG];
+    int dbins[kMaxDur];
+    double dur[kMaxDur];
+    int L[kWarps][kMaxDur];
+    longlong2 scan[kWarps];
+    float num[kWarps];
+    float den[kWarps];
+    int key[kWarps];
+    long long tile;
+    long long pb, pe, pn;
+    int curve;
+    int G;
+    int total;
+    int glob;
+};
+
+template <int GEOM>
+__device__ __forceinline__ int fold_slot(double d, double P, double IP, double k_bins, int NB) {
+    if (GEOM == ATB_GEOM_BINNED) return fold_binned(d, P, IP, k_bins, NB);
+    return fold_fixed(d, IP, k_bins, NB);
+}
+
+// fold every staged point of the curve into the group's histograms
+template <int GEOM, bool GLOB>
+__device__ void fold_group(const SearchArgs& a, const GroupSmem& gs, longlong2* H, long long so,
+                           long long n_pad, double k_bins_binned) {
+    const int G = gs.G;
+    for (long long base = 0; base < n_pad; base += (long long)kBlock * kR) {
+        const long long i0 = base + (long long)threadIdx.x * kR;
+        if (i0 >= n_pad) continue;
+        double d[kR];
+        int qw[kR], qy[kR];
+        const double2* dp = reinterpret_cast<const double2*>(a.sdt + so + i0);
+#pragma unroll
+        for (int q = 0; q < kR / 2; ++q) {
+            const double2 v = __ldg(dp + q);
+            d[2 * q] = v.x;
+            d[2 * q + 1] = v.y;
+        }
+        const int4* wp = reinterpret_cast<const int4*>(a.sqw + so + i0);
+        const int4* yp = reinterpret_cast<const int4*>(a.sqy + so + i0);
+#pragma unroll
+        for (int q = 0; q < kR / 4; ++q) {
+            const int4 vw = __ldg(wp + q);
+            const int4 vy = __ldg(yp + q);
+            qw[4 * q] = vw.x; qw[4 * q + 1] = vw.y; qw[4 * q + 2] = vw.z; qw[4 * q + 3] = vw.w;
+            qy[4 * q] = vy.x; qy[4 * q + 1] = vy.y; qy[4 * q + 2] = vy.z; qy[4 * q + 3] = vy.w;
+        }
+        for (int g = 0; g < G; ++g) {
+            const double P = gs.P[g];
+            const double IP = gs.IP[g];
+            const int NB = gs.NB[g];
+            const double kb = (GEOM == ATB_GEOM_BINNED) ? k_bins_binned : (double)NB;
+            longlong2* Hg = H + gs.base[g];
+            int cur = fold_slot<GEOM>(d[0], P, IP, kb, NB);
+            int aw = qw[0], ay = qy[0];
+#pragma unroll
+            for (int j = 1; j < kR; ++j) {
+                const int s = fold_slot<GEOM>(d[j], P, IP, kb, NB);
+                if (s != cur) {
+                    hist_add<GLOB>(Hg, cur, aw, ay);
+                    cur = s;
+                    aw = 0;
+                    ay = 0;
+                }
+                aw += qw[j];
+                ay += qy[j];
+            }
+            hist_add<GLOB>(Hg, cur, aw, ay);
+        }
+    }
+}
+
+// FP64 statistics of the winning window (exact quantised sums)
+__device__ void window_stats(double dw, double dy, double wtot, double ytot, int s_w, int s_y,
+                             int objective, double* power, double* depth, double* derr) {
+    const double w_in = ldexp(dw, -s_w);
+    const double w_out = ldexp(wtot - dw, -s_w);
+    const double s_in = ldexp(dy, -s_y);
+    const double s_out = ldexp(ytot - dy, -s_y);
+    const double y_in = s_in / w_in;
+    const double y_out = s_out / w_out;
+    const double dep = y_out - y_in;
+    const double de = sqrt(1.0 / w_in + 1.0 / w_out);
+    double pw;
+    if (objective == ATB_OBJ_FAST) {
+        pw = sqrt(dep * dep * (w_in * w_out));
+    } else if (objective == ATB_OBJ_LIKELIHOOD) {
+        pw = 0.5 * dep * dep * (w_in * w_out) / (w_in + w_out);
+    } else {
+        pw = dep / de;
+    }
+    *power = pw > 0.0 ? pw : 0.0;
+    *depth = dep;
+    *derr = de;
+}
+
+// exclusive->inclusive scan of H[0..M) in place, int64 -> exact FP64 bit patterns
+__device__ void team_scan(const Team& tm, GroupSmem& gs, longlong2* E, int M) {
+    const int seg = (M + tm.nthreads - 1) / tm.nthreads;
+    const int b = min(M, tm.tid * seg);
+    const int e = min(M, b + seg);
+    long long sw = 0, sy = 0;
+    for (int i = b; i < e; ++i) {
+        const longlong2 v = E[i];
+        sw += v.x;
+        sy += v.y;
+    }
+    const int lane = threadIdx.x & 31;
+    long long iw = sw, iy = sy;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const long long tw = __shfl_up_sync(0xffffffffu, iw, off);
+        const long long ty = __shfl_up_sync(0xffffffffu, iy, off);
+        if (lane >= off) {
+            iw += tw;
+            iy += ty;
+        }
+    }
+    if (tm.nwarps > 1) {
+        const int wl = (threadIdx.x >> 5) - tm.warp0;
+        if (lane == 31) gs.scan[tm.warp0 + wl] = make_longlong2(iw, iy);
+        team_sync(tm);
+        long long ow = 0, oy = 0;
+        for (int k = 0; k < wl; ++k) {
+            const longlong2 v = gs.scan[tm.warp0 + k];
+            ow += v.x;
+            oy += v.y;
+        }
+        iw += ow;
+        iy += oy;
+    }
+    long long xw = iw - sw, xy = iy - sy;
+    for (int i = b; i < e; ++i) {
+        const longlong2 v = E[i];
+        xw += v.x;
+        xy += v.y;
+        E[i] = make_longlong2(__double_as_longlong((double)xw), __double_as_longlong((double)xy));
+    }
+    team_sync(tm);
+}
+
+__device__ Cand team_best(const Team& tm, GroupSmem& gs, Cand c) {
+    c = warp_best(c);
+    if (tm.nwarps > 1) {
+        const int lane = threadIdx.x & 31;
+        const int wg = threadIdx.x >> 5;
+        if (lane == 0) {
+            gs.num[wg] = c.num;
+            gs.den[wg] = c.den;
+            gs.key[wg] = c.key;
+        }
+        team_sync(tm);
+        if (tm.tid == 0) {
+            for (int k = 1; k < tm.nwarps; ++k) {
+                const int j = tm.warp0 + k;
+                if (cand_better(gs.num[j], gs.den[j], gs.key[j], c.num, c.den, c.key)) {
+                    c.num = gs.num[j];
+                    c.den = gs.den[j];
+                    c.key = gs.key[j];
+                }
+            }
+        }
+        team_sync(tm);
+    }
+    return c;
+}
+
+template <int GEOM>
+__device__ void finalize_period(const SearchArgs& a, GroupSmem& gs, const Team& tm, longlong2* H,
+                                int g, const CurveStat& st, int nd) {
+    longlong2* E = H + gs.base[g];
+    const int NB = gs.NB[g];
+    const double P = gs.P[g];
+    const double IP = gs.IP[g];
+
+    if (GEOM == ATB_GEOM_BINNED) {
+        // padding copy, vbls_v42_parity.cu:78-80 (sequential semantics)
+        if (tm.tid == 0) {
+            for (int j = 1, ind = NB - a.oversample; j <= a.oversample; ++j, ++ind) E[ind] = E[j];
+        }
+        team_sync(tm);
+    } else {
+        if (tm.tid < nd) {
+            int L = (int)fma(gs.dur[tm.tid] * IP, (double)NB, 0.5);
+            if (L < 1) L = 1;
+            gs.L[tm.id][tm.tid] = L;
+        }
+    }
+    team_scan(tm, gs, E, NB + 1);
+
+    const double ay = st.qy_abs > 0 ? (double)st.qy_abs : 1.0;
+    const float ks = (float)(1.0 / ay);
+    double wtot, ytot;
+    if (GEOM == ATB_GEOM_BINNED) {
+        wtot = (double)st.qw_tot;
+        ytot = (double)st.qy_tot;
+    } else {
+        const longlong2 te = E[NB];
+        wtot = ll_as_d(te.x);
+        ytot = ll_as_d(te.y);
+    }
+    Cand best{-1.0f, 1.0f, 0x7fffffff};
+    if (wtot > 0.0) {
+        const float invw = (float)(1.0 / wtot);
+        const float stot = (float)(ytot / ay);
+        if (GEOM == ATB_GEOM_BINNED) {
+            const double thr = ldexp(1e-15, st.s_w);
+            for (int s = tm.tid; s < NB; s += tm.nthreads) {
+                const longlong2 e0 = E[s];
+                const double c0w = ll_as_d(e0.x), c0y = ll_as_d(e0.y);
+                for (int k = 0; k < nd; ++k) {
+                    const int dd = gs.dbins[k];
+                    if (s + dd > NB) continue;
+                    const longlong2 e1 = E[s + dd];
+                    const double dw = ll_as_d(e1.x) - c0w;
+                    const double dy = ll_as_d(e1.y) - c0y;
+                    const double wo = wtot - dw;
+                    if (dw < thr || wo < thr) continue;
+                    const float u = __fmul_rn(__double2float_rn(dw), invw);
+                    const float v = __fmul_rn(__double2float_rn(wo), invw);
+                    const float av = __fmul_rn(__double2float_rn(dy), ks);
+                    const float sig = __fmaf_rn(stot, u, -av);
+                    if (!(sig >= 0.0f)) continue;
+                    cand_consider(best, __fmul_rn(sig, sig), __fmul_rn(u, v), s * nd + k);
+                }
+            }
+        } else {
+            for (int s = tm.tid; s < NB; s += tm.nthreads) {
+                const longlong2 e0 = E[s];
+                const double c0w = ll_as_d(e0.x), c0y = ll_as_d(e0.y);
+                for (int k = 0; k < nd; ++k) {
+                    const int L = gs.L[tm.id][k];
+                    if (L >= NB) continue;
+                    double dw, dy;
+                    if (s + L <= NB) {
+                        const longlong2 e1 = E[s + L];
+                        dw = ll_as_d(e1.x) - c0w;
+                        dy = ll_as_d(e1.y) - c0y;
+                    } else {
+                        const longlong2 e1 = E[s + L - NB];
+                        dw = (wtot - c0w) + ll_as_d(e1.x);
+                        dy = (ytot - c0y) + ll_as_d(e1.y);
+                    }
+                    if (!(dw > 0.0 && dw < wtot)) continue;
+                    const float u = __fmul_rn(__double2float_rn(dw), invw);
+                    const float v = __fmul_rn(__double2float_rn(wtot - dw), invw);
+                    const float av = __fmul_rn(__double2float_rn(dy), ks);
+                    const float sig = __fmaf_rn(stot, u, -av);
+                    cand_consider(best, __fmul_rn(sig, sig), __fmul_rn(u, v), s * nd + k);
+                }
+            }
+        }
+    }
+    best = team_best(tm, gs, best);
+
+    if (tm.tid == 0) {
+        const long long slot = gs.slot[g];
+        float o_pw = 0.0f, o_dep = 0.0f, o_de = 0.0f, o_dur = 0.0f;
+        double o_t0 = 0.0;
+        int o_win = -1;
+        if (best.key != 0x7fffffff) {
+            const int s = best.key / nd, k = best.key % nd;
+            double dw, dy;
+            if (GEOM == ATB_GEOM_BINNED) {
+                const int dd = gs.dbins[k];
+                dw = ll_as_d(E[s + dd].x) - ll_as_d(E[s].x);
+                dy = ll_as_d(E[s + dd].y) - ll_as_d(E[s].y);
+                const double durv = (double)dd * st.bin_dur;
+                o_dur = (float)durv;
+                o_t0 = fmod((double)s * st.bin_dur + 0.5 * durv + st.t_start, P);
+            } else {
+                const int L = gs.L[tm.id][k];
+                if (s + L <= NB) {
+                    dw = ll_as_d(E[s + L].x) - ll_as_d(E[s].x);
+                    dy = ll_as_d(E[s + L].y) - ll_as_d(E[s].y);
+                } else {
+                    dw = (wtot - ll_as_d(E[s].x)) + ll_as_d(E[s + L - NB].x);
+                    dy = (ytot - ll_as_d(E[s].y)) + ll_as_d(E[s + L - NB].y);
+                }
+                o_dur = (float)gs.dur[k];
+                o_t0 = fma((double)s / (double)NB, 1.0 / IP, st.t_start);
+            }
+            double pw, dep, de;
+            window_stats(dw, dy, wtot, ytot, st.s_w, st.s_y, a.objective, &pw, &dep, &de);
+            o_pw = (float)pw;
+            o_dep = (float)dep;
+            o_de = (float)de;
+            o_win = best.key;
+        }
+        a.power[slot] = o_pw;
+        if (a.depth) a.depth[slot] = o_dep;
+        if (a.depth_err) a.depth_err[slot] = o_de;
+        if (a.t0) a.t0[slot] = o_t0;
+        if (a.duration) a.duration[slot] = o_dur;
+        if (a.window) a.window[slot] = o_win;
+    }
+    team_sync(tm);  // per-team scratch (window lengths, scan totals) is reused by the next period
+}
+
+template <int GEOM, bool GLOB>
+__device__ void run_group(const SearchArgs& a, GroupSmem& gs, longlong2* H, const CurveStat& st,
+                          long long so, long long n_pad, int nd) {
+    const int total = gs.total;
+    for (int i = threadIdx.x; i < total; i += kBlock) H[i] = make_longlong2(0, 0);
+    __syncthreads();
+    fold_group<GEOM, GLOB>(a, gs, H, so, n_pad, st.inv_bin_dur);
+    __syncthreads();
+    const int G = gs.G;
+    int tw = 1;
+    while (tw * 2 * G <= kWarps) tw *= 2;
+    const int n_teams = kWarps / tw;
+    const int warp = threadIdx.x >> 5;
+    Team tm;
+    tm.id = warp / tw;
+    tm.nwarps = tw;
+    tm.nthreads = tw * 32;
+    tm.warp0 = tm.id * tw;
+    tm.tid = threadIdx.x - tm.warp0 * 32;
+    for (int g = tm.id; g < G; g += n_teams) finalize_period<GEOM>(a, gs, tm, H, g, st, nd);
+    __syncthreads();
+}
+
+template <int GEOM>
+__global__ void __launch_bounds__(kBlock, 1) search_kernel(const SearchArgs a) {
+    extern __shared__ __align__(16) longlong2 s_hist[];
+    __shared__ GroupSmem gs;
+
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const long long tile = (long long)atomicAdd(a.tile_counter, 1ULL);
+            gs.tile = tile;
+            if (tile < a.n_tiles) {
+                int lo = 0, hi = a.n_curves;
+                while (hi - lo > 1) {
+                    const int mid = (lo + hi) >> 1;
+                    if (a.tile_off[mid] <= tile) lo = mid; else hi = mid;
+                }
+                const int c = a.order[lo];
+                gs.curve = c;
+                gs.pb = (tile - a.tile_off[lo]) * kTileP;
+                gs.pe = min(gs.pb + kTileP, a.per_cnt[c]);
+            }
+        }
+        __syncthreads();
+        if (gs.tile >= a.n_tiles) break;
+
+        const int c = gs.curve;
+        const CurveStat st = a.stats[c];
+        const int nd = a.dur_cnt[c];
+        const long long n = a.pt_off[c + 1] - a.pt_off[c];
+        const long long n_pad = (n + kR - 1) / kR * kR;
+        const long long so = a.stage_off[c];
+        const long long pbeg = a.per_beg[c];
+        const long long obeg = a.out_beg[c];
+        if (threadIdx.x < nd) {
+            gs.dbins[threadIdx.x] = a.dbins[c * kMaxDur + threadIdx.x];
+            gs.dur[threadIdx.x] = a.durations[a.dur_beg[c] + threadIdx.x];
+        }
+        long long pn = gs.pb;
+        const long long pe = gs.pe;
+        while (pn < pe) {
+            if (threadIdx.x == 0) {
+                int g = 0, base = 0;
+                long long p = pn;
+                while (p < pe && g < kMaxG) {
+                    double P = a.periods[pbeg + p];
+                    if (!(P > 0.0) || !(P < 1.0e300)) {
+                        atomicOr(a.status, 4);
+                        P = 1.0;
+                    }
+                    const int NB = (GEOM == ATB_GEOM_BINNED)
+                                       ? binned_nbins(P, st.inv_bin_dur, a.oversample, a.max_bins)
+                                       : a.n_bins_fixed;
+                    const int need = NB + 2;
+                    if (g > 0 && base + need > a.cap) break;
+                    gs.P[g] = P;
+                    gs.IP[g] = 1.0 / P;
+                    gs.NB[g] = NB;
+                    gs.base[g] = base;
+                    gs.slot[g] = obeg + p;
+                    base += need;
+                    ++g;
+                    ++p;
+                    if (base > a.cap) break;  // a lone oversized period: global histogram
+                }
+                gs.G = g;
+                gs.total = base;
+                gs.glob = base > a.cap ? 1 : 0;
+            }
+            __syncthreads();
+            if (gs.glob) {
+                run_group<GEOM, true>(a, gs, a.ghist + (long long)blockIdx.x * a.ghist_stride, st,
+                                      so, n_pad, nd);
+            } else {
+                run_group<GEOM, false>(a, gs, s_hist, st, so, n_pad, nd);
+            }
+            pn += gs.G;
+            __syncthreads();
+        }
+    }
+}
+
+// per-curve argmax over the grid (first maximum, as cupy.argmax)
+__global__ void best_kernel(int n_curves, const long long* per_cnt, const long long* out_beg,
+                            const float* power, int* best) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= n_curves) return;
+    const long long cnt = per_cnt[warp];
+    const float* pw = power + out_beg[warp];
+    float bv = -INFINITY;
+    long long bi = 0x7fffffffffffffffLL;
+    for (long long i = lane; i < cnt; i += 32) {
+        const float v = pw[i];
+        if (v > bv) { bv = v; bi = i; }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const float ov = __shfl_xor_sync(0xffffffffu, bv, off);
+        const long long oi = __shfl_xor_sync(0xffffffffu, bi, off);
+        if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+    }
+    if (lane == 0) best[warp] = cnt > 0 ? (int)bi : -1;
+}
+
+// per-point histogram slots of curve 0 for every period (verification only)
+template <int GEOM>
+__global__ void debug_fold_kernel(const double* sdt, long long n, const CurveStat* stats,
+                                  const double* periods, long long n_periods, int oversample,
+                                  int max_bins, int n_bins_fixed, int* out) {
+    const long long total = n * n_periods;
+    const CurveStat st = stats[0];
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const long long p = idx / n, i = idx % n;
+        const double P = periods[p];
+        const int NB = (GEOM == ATB_GEOM_BINNED)
+                           ? binned_nbins(P, st.inv_bin_dur, oversample, max_bins)
+                           : n_bins_fixed;
+        const double kb = (GEOM == ATB_GEOM_BINNED) ? st.inv_bin_dur : (double)NB;
+        out[idx] = fold_slot<GEOM>(sdt[i], P, 1.0 / P, kb, NB);
+    }
+}
+
+__global__ void nbins_max_kernel(int n_curves, const long long* per_beg, const long long* per_cnt,
+                                 const long long* dur_beg, const int* dur_cnt,
+                                 const double* periods, const double* durations, int oversample,
+                                 int max_bins, int* out) {
+    const int c = blockIdx.x;
+    if (c >= n_curves) return;
+    // same bin duration as the stage kernel
+    const double* dur = durations + dur_beg[c];
+    double min_dur = dur[0];
+    for (int k = 1; k < dur_cnt[c]; ++k) min_dur = min(min_dur, dur[k]);
+    const double ibd = 1.0 / (min_dur / (double)oversample);
+    int m = 0;
+    for (long long i = threadIdx.x; i < per_cnt[c]; i += blockDim.x) {
+        double P = periods[per_beg[c] + i];
+        if (!(P > 0.0) || !(P < 1.0e300)) P = 1.0;  // the search kernel's substitute
+        m = max(m, binned_nbins(P, ibd, oversample, max_bins));
+    }
+    m = warp_max(m);
+    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+// ----------------------------------------------------------------------------
+// microbenchmarks for the roofline denominators
+// ----------------------------------------------------------------------------
+
+constexpr int kBenchSlots = 4096;  // 32 KiB of u64 counters
+
+// 64-bit shared-memory reductions: pattern 0 = each warp's lanes hit 32
+// consecutive counters (conflict-free), pattern 1 = pseudo-random counters.
+__global__ void __launch_bounds__(kBlock) bench_smem_red_kernel(int iters, int pattern,
+                                                                unsigned long long* sink) {
+    __shared__ unsigned long long h[kBenchSlots];
+    for (int i = threadIdx.x; i < kBenchSlots; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+    unsigned x = threadIdx.x * 2654435761u + blockIdx.x * 97u + 1u;
+    const unsigned base = (unsigned)__cvta_generic_to_shared(h);
+    for (int i = 0; i < iters; ++i) {
+        unsigned slot;
+        if (pattern == 0) {
+            slot = (threadIdx.x + (unsigned)i * 64u) & (kBenchSlots - 1);
+        } else {
+            x = x * 1664525u + 1013904223u;
+            slot = (x >> 9) & (kBenchSlots - 1);
+        }
+        asm volatile("red.shared.add.u64 [%0], %1;" ::"r"(base + slot * 8u), "l"(1ULL) : "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) atomicAdd(sink, h[blockIdx.x & (kBenchSlots - 1)]);
+}
+
+// FP64 fused multiply-add throughput: 8 independent chains per thread
+__global__ void __launch_bounds__(kBlock) bench_dfma_kernel(int iters, double* sink) {
+    double a[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[k] = 1.0 + 1e-9 * (threadIdx.x + k);
+    const double m = 0.9999999, c = 1e-7;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) a[k] = fma(a[k], m, c);
+    }
+    double r = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) r += a[k];
+    if (r == 12345.678) sink[0] = r;  // keeps the chains alive
+}
+
+}  // namespace
+
+// ============================================================================
+// host side
+// ============================================================================
+
+struct atb_handle {
+    int device = 0;
+    int n_sm = 0;
+    int smem_optin = 0;
+    std::string err;
+};
+
+struct atb_plan {
+    atb_handle* h = nullptr;
+    atb_params prm{};
+    int n_curves = 0;
+    int y_is_f64 = 0;
+    int grid = 0;
+    int smem_bytes = 0;
+    long long n_tiles = 0;
+    std::vector<void*> allocs;
+    long long scratch_bytes = 0;
+    StageArgs sa{};
+    SearchArgs qa{};
+    int* best = nullptr;
+    int* status = nullptr;
+    unsigned long long* counter = nullptr;
+};
+
+namespace {
+
+int fail(atb_handle* h, int code, const char* fmt, ...) {
+    if (h) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof buf, fmt, ap);
+        va_end(ap);
+        h->err = buf;
+    }
+    return code;
+}
+
+#define ATB_CUDA(h, call)                                                                      \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            return fail((h), e_ == cudaErrorMemoryAllocation ? ATB_ENOMEM : ATB_ECUDA,         \
+                        "%s: %s", #call, cudaGetErrorString(e_));                              \
+    } while (0)
+
+template <typename T>
+int plan_alloc(atb_plan* p, T** out, size_t count) {
+    void* ptr = nullptr;
+    const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    cudaError_t e = cudaMalloc(&ptr, bytes);
+    if (e != cudaSuccess)
+        return fail(p->h, ATB_ENOMEM, "cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(e));
+    p->allocs.push_back(ptr);
+    p->scratch_bytes += (long long)bytes;
+    *out = static_cast<T*>(ptr);
+    return ATB_OK;
+}
+
+template <typename T>
+int plan_upload(atb_plan* p, T** out, const std::vector<T>& host) {
+    int rc = plan_alloc(p, out, host.size());
+    if (rc) return rc;
+    if (!host.empty()) ATB_CUDA(p->h, cudaMemcpy(*out, host.data(), host.size() * sizeof(T),
+                                                 cudaMemcpyHostToDevice));
+    return ATB_OK;
+}
+
+void plan_free(atb_plan* p) {
+    for (void* q : p->allocs) cudaFree(q);
+    p->allocs.clear();
+}
+
+int launch_stage(atb_plan* p, cudaStream_t s) {
+    if (p->y_is_f64)
+        stage_kernel<double><<<p->n_curves, kStageBlock, 0, s>>>(p->sa);
+    else
+        stage_kernel<float><<<p->n_curves, kStageBlock, 0, s>>>(p->sa);
+    ATB_CUDA(p->h, cudaGetLastError());
+    return ATB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* atb_version(void) { return ATB_VERSION; }
+
+int atb_create(int device, atb_handle** out) {
+    if (!out) return ATB_EINVAL;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) return ATB_ECUDA;
+    atb_handle* h = new atb_handle();
+    h->device = device;
+    cudaSetDevice(device);
+    cudaDeviceGetAttribute(&h->n_sm, cudaDevAttrMultiProcessorCount, device);
+    cudaDeviceGetAttribute(&h->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    *out = h;
+    return ATB_OK;
+}
+
+void atb_destroy(atb_handle* h) { delete h; }
+
+int atb_last_error(const atb_handle* h, char* buf, size_t len) {
+    if (!h) return 0;
+    if (buf && len) {
+        std::strncpy(buf, h->err.c_str(), len - 1);
+        buf[len - 1] = '\0';
+    }
+    return (int)h->err.size();
+}
+
+int atb_plan_create(atb_handle* h, const atb_params* prm, const atb_batch* b,
+                    const atb_outputs* o, atb_plan** out) {
+    if (!h) return ATB_EINVAL;
+    if (!prm || !b || !o || !out) return fail(h, ATB_EINVAL, "null argument");
+    *out = nullptr;
+    h->err.clear();
+    const int nc = b->n_curves;
+    if (nc < 1) return fail(h, ATB_EINVAL, "n_curves must be >= 1");
+    if (prm->geometry == ATB_GEOM_FIXED) {
+        if (prm->objective != ATB_OBJ_FAST)
+            return fail(h, ATB_EINVAL, "the fixed-bin geometry uses the fast objective");
+        if (prm->n_bins < 2 || prm->n_bins > (1 << 24))
+            return fail(h, ATB_EINVAL, "n_bins=%d out of range [2, 2^24]", prm->n_bins);
+    } else if (prm->geometry == ATB_GEOM_BINNED) {
+        if (prm->objective != ATB_OBJ_SNR && prm->objective != ATB_OBJ_LIKELIHOOD)
+            return fail(h, ATB_EINVAL, "the binned geometry uses the snr or likelihood objective");
+        if (prm->oversample < 1 || prm->oversample > 1000)
+            return fail(h, ATB_EINVAL, "oversample=%d out of range [1, 1000]", prm->oversample);
+        if (prm->max_bins != 0 && prm->max_bins < prm->oversample + 2)
+            return fail(h, ATB_EINVAL, "max_bins=%d must be 0 or >= oversample+2", prm->max_bins);
+    } else {
+        return fail(h, ATB_EINVAL, "unknown geometry %d", prm->geometry);
+    }
+    if (!b->point_offset || !b->period_begin || !b->period_count || !b->dur_begin ||
+        !b->dur_count || !b->out_begin)
+        return fail(h, ATB_EINVAL, "batch index arrays must not be NULL");
+    if (!b->t || !b->y || !b->periods || !b->durations)
+        return fail(h, ATB_EINVAL, "batch data pointers must not be NULL");
+    if (!o->power) return fail(h, ATB_EINVAL, "outputs.power must not be NULL");
+
+    std::vector<long long> pt_off(nc + 1), t_off(nc), per_beg(nc), per_cnt(nc), dur_beg(nc),
+        out_beg(nc), stage_off(nc), tile_off(nc + 1);
+    std::vector<int> dur_cnt(nc), order(nc);
+    long long staged = 0, n_out_max = 0;
+    for (int c = 0; c <= nc; ++c) pt_off[c] = b->point_offset[c];
+    for (int c = 0; c < nc; ++c) {
+        const long long n = pt_off[c + 1] - pt_off[c];
+        if (n < 0) return fail(h, ATB_EINVAL, "curve %d: decreasing point_offset", c);
+        if (n > (1LL << 26)) return fail(h, ATB_EINVAL, "curve %d: more than 2^26 points", c);
+        t_off[c] = b->time_offset ? b->time_offset[c] : pt_off[c];
+        per_beg[c] = b->period_begin[c];
+        per_cnt[c] = b->period_count[c];
+        dur_beg[c] = b->dur_begin[c];
+        dur_cnt[c] = b->dur_count[c];
+        out_beg[c] = b->out_begin[c];
+        if (per_cnt[c] < 0 || per_beg[c] < 0 || out_beg[c] < 0 || dur_beg[c] < 0)
+            return fail(h, ATB_EINVAL, "curve %d: negative grid index", c);
+        if (per_cnt[c] > (1LL << 30)) return fail(h, ATB_EINVAL, "curve %d: too many periods", c);
+        if (dur_cnt[c] < 1 || dur_cnt[c] > kMaxDur)
+            return fail(h, ATB_EINVAL, "curve %d: dur_count=%d outside [1, %d]", c, dur_cnt[c],
+                        kMaxDur);
+        stage_off[c] = staged;
+        staged += (n + kR - 1) / kR * kR;
+        staged = (staged + kStageAlign - 1) / kStageAlign * kStageAlign;
+        n_out_max = std::max(n_out_max, out_beg[c] + per_cnt[c]);
+    }
+    // largest-first schedule of curves (cost ~ points x periods)
+    for (int c = 0; c < nc; ++c) order[c] = c;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        const double cx = (double)(pt_off[x + 1] - pt_off[x] + 64) * (double)per_cnt[x];
+        const double cy = (double)(pt_off[y + 1] - pt_off[y] + 64) * (double)per_cnt[y];
+        return cx > cy;
+    });
+    tile_off[0] = 0;
+    for (int j = 0; j < nc; ++j)
+        tile_off[j + 1] = tile_off[j] + (per_cnt[order[j]] + kTileP - 1) / kTileP;
+
+    ATB_CUDA(h, cudaSetDevice(h->device));
+    atb_plan* p = new atb_plan();
+    p->h = h;
+    p->prm = *prm;
+    p->n_curves = nc;
+    p->y_is_f64 = b->y_is_f64 ? 1 : 0;
+    p->n_tiles = tile_off[nc];
+
+    int rc = ATB_OK;
+    long long *d_pt, *d_toff, *d_pbeg, *d_pcnt, *d_dbeg, *d_obeg, *d_soff, *d_tiles;
+    int *d_dcnt, *d_order, *d_dbins;
+    double* d_sdt;
+    int *d_sqw, *d_sqy;
+    CurveStat* d_stats;
+    if ((rc = plan_upload(p, &d_pt, pt_off)) || (rc = plan_upload(p, &d_toff, t_off)) ||
+        (rc = plan_upload(p, &d_pbeg, per_beg)) || (rc = plan_upload(p, &d_pcnt, per_cnt)) ||
+        (rc = plan_upload(p, &d_dbeg, dur_beg)) || (rc = plan_upload(p, &d_obeg, out_beg)) ||
+        (rc = plan_upload(p, &d_soff, stage_off)) || (rc = plan_upload(p, &d_tiles, tile_off)) ||
+        (rc = plan_upload(p, &d_dcnt, dur_cnt)) || (rc = plan_upload(p, &d_order, order)) ||
+        (rc = plan_alloc(p, &d_dbins, (size_t)nc * kMaxDur)) ||
+        (rc = plan_alloc(p, &d_sdt, (size_t)staged)) || (rc = plan_alloc(p, &d_sqw, (size_t)staged)) ||
+        (rc = plan_alloc(p, &d_sqy, (size_t)staged)) || (rc = plan_alloc(p, &d_stats, (size_t)nc)) ||
+        (rc = plan_alloc(p, &p->status, 1)) || (rc = plan_alloc(p, &p->counter, 1))) {
+        plan_free(p);
+        delete p;
+        return rc;
+    }
+
+    StageArgs& sa = p->sa;
+    sa.pt_off = d_pt;
+    sa.t_off = d_toff;
+    sa.stage_off = d_soff;
+    sa.dur_beg = d_dbeg;
+    sa.dur_cnt = d_dcnt;
+    sa.t = b->t;
+    sa.y = b->y;
+    sa.w = b->w;
+    sa.durations = b->durations;
+    sa.sdt = d_sdt;
+    sa.sqw = d_sqw;
+    sa.sqy = d_sqy;
+    sa.stats = d_stats;
+    sa.dbins = d_dbins;
+    sa.oversample = prm->geometry == ATB_GEOM_BINNED ? prm->oversample : 1;
+    sa.status = p->status;
+
+    // shared-memory histogram capacity and the global fallback size
+    const int static_smem = (int)sizeof(GroupSmem) + 64;
+    int dyn = h->smem_optin - static_smem - 1024;
+    dyn = dyn / 16 * 16;
+    const int cap = dyn / 16;
+    int nb_max = prm->n_bins;
+    if (prm->geometry == ATB_GEOM_BINNED) {
+        // largest bin count over the batch sizes the global-histogram fallback
+        int* d_nb = nullptr;
+        if ((rc = plan_alloc(p, &d_nb, 1))) { plan_free(p); delete p; return rc; }
+        cudaMemset(d_nb, 0, sizeof(int));
+        nbins_max_kernel<<<nc, 256>>>(nc, d_pbeg, d_pcnt, d_dbeg, d_dcnt, b->periods,
+                                      b->durations, prm->oversample, prm->max_bins, d_nb);
+        cudaError_t e = cudaMemcpy(&nb_max, d_nb, sizeof(int), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) {
+            plan_free(p);
+            delete p;
+            return fail(h, ATB_ECUDA, "n_bins reduction: %s", cudaGetErrorString(e));
+        }
+        int nd_max = 1;
+        for (int c = 0; c < nc; ++c) nd_max = std::max(nd_max, dur_cnt[c]);
+        if (nb_max >= (1 << 27) || (long long)nb_max * nd_max >= (1LL << 31)) {
+            plan_free(p);
+            delete p;
+            return fail(h, ATB_EINVAL, "a period needs %d bins (limit 2^27 and bins x durations < 2^31)",
+                        nb_max);
+        }
+    }
+    int occ = 1;
+    cudaError_t e0 = cudaSuccess;
+    if (prm->geometry == ATB_GEOM_BINNED)
+        e0 = cudaFuncSetAttribute(search_kernel<ATB_GEOM_BINNED>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+    else
+        e0 = cudaFuncSetAttribute(search_kernel<ATB_GEOM_FIXED>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+    if (e0 != cudaSuccess) {
+        plan_free(p);
+        delete p;
+        return fail(h, ATB_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e0));
+    }
+    if (prm->geometry == ATB_GEOM_BINNED)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, search_kernel<ATB_GEOM_BINNED>, kBlock, dyn);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, search_kernel<ATB_GEOM_FIXED>, kBlock, dyn);
+    occ = std::max(occ, 1);
+    long long grid = (long long)h->n_sm * occ;
+    grid = std::max(1LL, std::min(grid, p->n_tiles));
+    p->grid = (int)grid;
+    p->smem_bytes = dyn;
+
+    longlong2* d_ghist = nullptr;
+    long long gstride = 0;
+    if (nb_max + 2 > cap) {
+        gstride = ((long long)nb_max + 2 + 15) / 16 * 16;
+        const long long bytes = gstride * 16 * grid;
+        if (bytes > (16LL << 30)) {
+            plan_free(p);
+            delete p;
+            return fail(h, ATB_EINVAL, "global histograms would need %lld bytes", bytes);
+        }
+        if ((rc = plan_alloc(p, &d_ghist, (size_t)(gstride * grid)))) {
+            plan_free(p);
+            delete p;
+            return rc;
+        }
+    }
+
+    SearchArgs& qa = p->qa;
+    qa.objective = prm->objective;
+    qa.n_bins_fixed = prm->n_bins;
+    qa.oversample = sa.oversample;
+    qa.max_bins = prm->max_bins;
+    qa.n_curves = nc;
+    qa.cap = cap;
+    qa.n_tiles = p->n_tiles;
+    qa.pt_off = d_pt;
+    qa.stage_off = d_soff;
+    qa.per_beg = d_pbeg;
+    qa.per_cnt = d_pcnt;
+    qa.dur_beg = d_dbeg;
+    qa.dur_cnt = d_dcnt;
+    qa.out_beg = d_obeg;
+    qa.tile_off = d_tiles;
+    qa.order = d_order;
+    qa.periods = b->periods;
+    qa.durations = b->durations;
+    qa.sdt = d_sdt;
+    qa.sqw = d_sqw;
+    qa.sqy = d_sqy;
+    qa.stats = d_stats;
+    qa.dbins = d_dbins;
+    qa.power = o->power;
+    qa.depth = o->depth;
+    qa.depth_err = o->depth_err;
+    qa.t0 = o->t0;
+    qa.duration = o->duration;
+    qa.window = o->window;
+    qa.ghist = d_ghist;
+    qa.ghist_stride = gstride;
+    qa.tile_counter = p->counter;
+    qa.status = p->status;
+    p->best = o->best_period;
+    ATB_CUDA(h, cudaDeviceSynchronize());
+    *out = p;
+    return ATB_OK;
+}
+
+int atb_plan_execute(atb_plan* p, void* stream) {
+    if (!p) return ATB_EINVAL;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    atb_handle* h = p->h;
+    ATB_CUDA(h, cudaMemsetAsync(p->counter, 0, sizeof(unsigned long long), s));
+    ATB_CUDA(h, cudaMemsetAsync(p->status, 0, sizeof(int), s));
+    int rc = launch_stage(p, s);
+    if (rc) return rc;
+    if (p->n_tiles > 0) {
+        if (p->prm.geometry == ATB_GEOM_BINNED)
+            search_kernel<ATB_GEOM_BINNED><<<p->grid, kBlock, p->smem_bytes, s>>>(p->qa);
+        else
+            search_kernel<ATB_GEOM_FIXED><<<p->grid, kBlock, p->smem_bytes, s>>>(p->qa);
+        ATB_CUDA(h, cudaGetLastError());
+    }
+    if (p->best) {
+        const int threads = 256;
+        const int blocks = (p->n_curves * 32 + threads - 1) / threads;
+        best_kernel<<<blocks, threads, 0, s>>>(p->n_curves, p->qa.per_cnt, p->qa.out_beg,
+                                               p->qa.power, p->best);
+        ATB_CUDA(h, cudaGetLastError());
+    }
+    return ATB_OK;
+}
+
+int atb_plan_kernel_count(const atb_plan* p) {
+    if (!p) return 0;
+    return 1 + (p->n_tiles > 0 ? 1 : 0) + (p->best ? 1 : 0);
+}
+
+int64_t atb_plan_scratch_bytes(const atb_plan* p) { return p ? p->scratch_bytes : 0; }
+
+int atb_plan_check(atb_plan* p) {
+    if (!p) return ATB_EINVAL;
+    int st = 0;
+    ATB_CUDA(p->h, cudaMemcpy(&st, p->status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (st & 1) return fail(p->h, ATB_EDATA, "input contains non-finite values or weights <= 0");
+    if (st & 2) return fail(p->h, ATB_EDATA, "durations must be positive and finite");
+    if (st & 4) return fail(p->h, ATB_EDATA, "periods must be positive and finite");
+    return ATB_OK;
+}
+
+void atb_plan_destroy(atb_plan* p) {
+    if (!p) return;
+    cudaSetDevice(p->h->device);
+    plan_free(p);
+    delete p;
+}
+
+int atb_search(atb_handle* h, const atb_params* prm, const atb_batch* b, const atb_outputs* o,
+               void* stream) {
+    atb_plan* p = nullptr;
+    int rc = atb_plan_create(h, prm, b, o, &p);
+    if (rc) return rc;
+    rc = atb_plan_execute(p, stream);
+    if (!rc) {
+        cudaError_t e = cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+        if (e != cudaSuccess) rc = fail(h, ATB_ECUDA, "search: %s", cudaGetErrorString(e));
+    }
+    if (!rc) rc = atb_plan_check(p);
+    atb_plan_destroy(p);
+    return rc;
+}
+
+int atb_run_gpu_bls(atb_handle* h, const double* t, const float* y, const float* w, int64_t n,
+                    const double* periods, int64_t n_periods, const double* durations,
+                    int32_t n_durations, int32_t n_bins, float* power, double* t0,
+                    float* duration, float* depth, int32_t* best_index, void* stream) {
+    if (!h) return ATB_EINVAL;
+    atb_params prm{ATB_GEOM_FIXED, ATB_OBJ_FAST, n_bins, 10, 0, 0};
+    const int64_t pt[2] = {0, n};
+    const int64_t zero = 0;
+    const int64_t pc = n_periods;
+    const int32_t dc = n_durations;
+    atb_batch b{};
+    b.n_curves = 1;
+    b.point_offset = pt;
+    b.period_begin = &zero;
+    b.period_count = &pc;
+    b.dur_begin = &zero;
+    b.dur_count = &dc;
+    b.out_begin = &zero;
+    b.t = t;
+    b.y = y;
+    b.w = w;
+    b.periods = periods;
+    b.durations = durations;
+    int32_t* d_best = nullptr;
+    if (best_index) {
+        ATB_CUDA(h, cudaMalloc(&d_best, sizeof(int32_t)));
+    }
+    atb_outputs o{};
+    o.power = power;
+    o.t0 = t0;
+    o.duration = duration;
+    o.depth = depth;
+    o.best_period = d_best;
+    int rc = atb_search(h, &prm, &b, &o, stream);
+    if (!rc && best_index) {
+        cudaError_t e = cudaMemcpy(best_index, d_best, sizeof(int32_t), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) rc = fail(h, ATB_ECUDA, "best index: %s", cudaGetErrorString(e));
+    }
+    if (d_best) cudaFree(d_best);
+    return rc;
+}
+
+int atb_run_vbls_exact_parity(atb_handle* h, const double* time, const float* flux,
+                              const float* weights, int64_t n_targets, int64_t n_data,
+                              const double* periods, int64_t n_periods, const double* durations,
+                              int32_t n_durations, int32_t oversample, int32_t max_bins,
+                              int32_t objective, float* power, double* t0, float* duration,
+                              float* depth, int32_t* best_index, void* stream) {
+    if (!h) return ATB_EINVAL;
+    if (n_targets < 1 || n_targets > (1 << 30)) return fail(h, ATB_EINVAL, "n_targets out of range");
+    atb_params prm{ATB_GEOM_BINNED, objective, 0, oversample, max_bins, 0};
+    const int nc = (int)n_targets;
+    std::vector<int64_t> pt(nc + 1), toff(nc, 0), pbeg(nc, 0), pcnt(nc, n_periods), dbeg(nc, 0),
+        obeg(nc);
+    std::vector<int32_t> dcnt(nc, n_durations);
+    for (int c = 0; c <= nc; ++c) pt[c] = (int64_t)c * n_data;
+    for (int c = 0; c < nc; ++c) obeg[c] = (int64_t)c * n_periods;
+    atb_batch b{};
+    b.n_curves = nc;
+    b.point_offset = pt.data();
+    b.time_offset = toff.data();
+    b.period_begin = pbeg.data();
+    b.period_count = pcnt.data();
+    b.dur_begin = dbeg.data();
+    b.dur_count = dcnt.data();
+    b.out_begin = obeg.data();
+    b.t = time;
+    b.y = flux;
+    b.w = weights;
+    b.periods = periods;
+    b.durations = durations;
+    atb_outputs o{};
+    o.power = power;
+    o.t0 = t0;
+    o.duration = duration;
+    o.depth = depth;
+    o.best_period = best_index;
+    return atb_search(h, &prm, &b, &o, stream);
+}
+
+int atb_debug_fold(atb_handle* h, const atb_params* prm, const double* t, const float* y,
+                   const float* w, int64_t n, const double* periods, int64_t n_periods,
+                   const double* durations, int32_t n_durations, int32_t* out_slots,
+                   void* stream) {
+    if (!h) return ATB_EINVAL;
+    if (!prm || !out_slots || n < 1 || n_periods < 1) return fail(h, ATB_EINVAL, "bad arguments");
+    const int64_t pt[2] = {0, n};
+    const int64_t zero = 0;
+    const int64_t pc = n_periods;
+    const int32_t dc = n_durations;
+    atb_batch b{};
+    b.n_curves = 1;
+    b.point_offset = pt;
+    b.period_begin = &zero;
+    b.period_count = &pc;
+    b.dur_begin = &zero;
+    b.dur_count = &dc;
+    b.out_begin = &zero;
+    b.t = t;
+    b.y = y;
+    b.w = w;
+    b.periods = periods;
+    b.durations = durations;
+    float* tmp = nullptr;
+    ATB_CUDA(h, cudaMalloc(&tmp, sizeof(float) * (size_t)n_periods));
+    atb_outputs o{};
+    o.power = tmp;
+    atb_plan* p = nullptr;
+    int rc = atb_plan_create(h, prm, &b, &o, &p);
+    if (!rc) {
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        rc = launch_stage(p, s);
+        if (!rc) {
+            const long long total = (long long)n * n_periods;
+            const int blocks = (int)std::min<long long>((total + 255) / 256, 65535);
+            if (prm->geometry == ATB_GEOM_BINNED)
+                debug_fold_kernel<ATB_GEOM_BINNED><<<blocks, 256, 0, s>>>(
+                    p->sa.sdt, n, p->sa.stats, periods, n_periods, prm->oversample,
+                    prm->max_bins, prm->n_bins, out_slots);
+            else
+                debug_fold_kernel<ATB_GEOM_FIXED><<<blocks, 256, 0, s>>>(
+                    p->sa.sdt, n, p->sa.stats, periods, n_periods, prm->oversample,
+                    prm->max_bins, prm->n_bins, out_slots);
+            cudaError_t e = cudaStreamSynchronize(s);
+            if (e != cudaSuccess) rc = fail(h, ATB_ECUDA, "debug fold: %s", cudaGetErrorString(e));
+        }
+        atb_plan_destroy(p);
+    }
+    cudaFree(tmp);
+    return rc;
+}
+
+
+int atb_plan_profile(atb_plan* p, void* stream, float* ms_stage, float* ms_search,
+                     float* ms_best) {
+    if (!p) return ATB_EINVAL;
+    atb_handle* h = p->h;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaEvent_t ev[4];
+    for (auto& e : ev) ATB_CUDA(h, cudaEventCreate(&e));
+    ATB_CUDA(h, cudaMemsetAsync(p->counter, 0, sizeof(unsigned long long), s));
+    ATB_CUDA(h, cudaMemsetAsync(p->status, 0, sizeof(int), s));
+    ATB_CUDA(h, cudaEventRecord(ev[0], s));
+    int rc = launch_stage(p, s);
+    ATB_CUDA(h, cudaEventRecord(ev[1], s));
+    if (!rc && p->n_tiles > 0) {
+        if (p->prm.geometry == ATB_GEOM_BINNED)
+            search_kernel<ATB_GEOM_BINNED><<<p->grid, kBlock, p->smem_bytes, s>>>(p->qa);
+        else
+            search_kernel<ATB_GEOM_FIXED><<<p->grid, kBlock, p->smem_bytes, s>>>(p->qa);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) rc = fail(h, ATB_ECUDA, "search launch: %s", cudaGetErrorString(e));
+    }
+    ATB_CUDA(h, cudaEventRecord(ev[2], s));
+    if (!rc && p->best) {
+        const int blocks = (p->n_curves * 32 + 255) / 256;
+        best_kernel<<<blocks, 256, 0, s>>>(p->n_curves, p->qa.per_cnt, p->qa.out_beg,
+                                           p->qa.power, p->best);
+    }
+    ATB_CUDA(h, cudaEventRecord(ev[3], s));
+    ATB_CUDA(h, cudaEventSynchronize(ev[3]));
+    float m[3] = {0, 0, 0};
+    for (int k = 0; k < 3; ++k) cudaEventElapsedTime(&m[k], ev[k], ev[k + 1]);
+    for (auto& e : ev) cudaEventDestroy(e);
+    if (ms_stage) *ms_stage = m[0];
+    if (ms_search) *ms_search = m[1];
+    if (ms_best) *ms_best = m[2];
+    return rc;
+}
+
+int atb_bench_smem_red_u64(atb_handle* h, int pattern, double* reductions_per_s) {
+    if (!h || !reductions_per_s) return ATB_EINVAL;
+    ATB_CUDA(h, cudaSetDevice(h->device));
+    unsigned long long* sink = nullptr;
+    ATB_CUDA(h, cudaMalloc(&sink, sizeof(unsigned long long)));
+    const int iters = 4096, grid = h->n_sm * 2;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    bench_smem_red_kernel<<<grid, kBlock>>>(iters, pattern, sink);  // warm-up
+    cudaEventRecord(a);
+    for (int r = 0; r < 5; ++r) bench_smem_red_kernel<<<grid, kBlock>>>(iters, pattern, sink);
+    cudaEventRecord(b);
+    cudaError_t e = cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(sink);
+    if (e != cudaSuccess) return fail(h, ATB_ECUDA, "bench: %s", cudaGetErrorString(e));
+    *reductions_per_s = 5.0 * grid * kBlock * (double)iters / (ms * 1e-3);
+    return ATB_OK;
+}
+
+int atb_bench_dfma(atb_handle* h, double* fma_per_s) {
+    if (!h || !fma_per_s) return ATB_EINVAL;
+    ATB_CUDA(h, cudaSetDevice(h->device));
+    double* sink = nullptr;
+    ATB_CUDA(h, cudaMalloc(&sink, sizeof(double)));
+    const int iters = 8192, grid = h->n_sm * 4;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    bench_dfma_kernel<<<grid, kBlock>>>(iters, sink);
+    cudaEventRecord(a);
+    for (int r = 0; r < 5; ++r) bench_dfma_kernel<<<grid, kBlock>>>(iters, sink);
+    cudaEventRecord(b);
+    cudaError_t e = cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(sink);
+    if (e != cudaSuccess) return fail(h, ATB_ECUDA, "bench: %s", cudaGetErrorString(e));
+    *fma_per_s = 5.0 * grid * kBlock * 8.0 * (double)iters / (ms * 1e-3);
+    return ATB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,429 @@
+"""Batched BLS engine over device tensors.
+
+A :class:`CurveBatch` holds a ragged batch of light curves (each with its own
+length, period grid and duration grid) in device memory; :class:`BLSEngine`
+binds it to output tensors in a :class:`SearchPlan`, whose ``execute`` only
+enqueues the engine's kernels on a CUDA stream (no allocation, no host
+synchronisation, so it can be captured in a CUDA graph).
+
+PyTorch is used for device memory and streams only; all compute runs in the
+sm_100a kernels of ``libastrotransit_b200.so``.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Sequence
+
+import numpy as np
+import torch
+
+from . import _native as N
+
+
+@dataclass
+class SearchConfig:
+    """What to compute.
+
+    method     "fast"   -- fixed ``n_bins`` phase bins, two-sided score (bls.cu)
+               "parity" -- bin = min(duration)/oversample, dip-only (V42 kernel)
+    objective  "fast" for method="fast"; "snr" (reference) or "likelihood"
+               for method="parity"
+    max_bins   None = no cap; an int reproduces the reference's cap
+               n_bins = min(n_bins, max_bins-1) (vbls_v42_parity.cu:46-47)
+    """
+    method: str = "parity"
+    objective: Optional[str] = None
+    n_bins: int = 200
+    oversample: int = 10
+    max_bins: Optional[int] = None
+
+    def params(self) -> N.Params:
+        if self.method == "fast":
+            obj = self.objective or "fast"
+            if obj != "fast":
+                raise ValueError("method='fast' uses the reference's fast score")
+            return N.Params(N.GEOM_FIXED, N.OBJ_FAST, int(self.n_bins), int(self.oversample), 0, 0)
+        if self.method == "parity":
+            obj = self.objective or "snr"
+            if obj not in ("snr", "likelihood"):
+                raise ValueError("method='parity' supports objective 'snr' or 'likelihood'")
+            mb = 0 if self.max_bins is None else int(self.max_bins)
+            return N.Params(N.GEOM_BINNED, N.OBJECTIVES[obj], int(self.n_bins),
+                            int(self.oversample), mb, 0)
+        raise ValueError(f"unknown method {self.method!r} (expected 'fast' or 'parity')")
+
+
+def is_shared_grid(g) -> bool:
+    """True when ``g`` is one 1-D grid (rather than one grid per curve)."""
+    if isinstance(g, np.ndarray):
+        return g.ndim <= 1
+    try:
+        return np.asarray(g, dtype=np.float64).ndim <= 1
+    except (ValueError, TypeError):
+        return False
+
+
+def _i64(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.int64))
+
+
+def _i32(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.int32))
+
+
+@dataclass
+class CurveBatch:
+    """Ragged batch in device memory plus its host-side index arrays."""
+    t: torch.Tensor                 # float64 [sum n]  (or the shared axis, see time_offset)
+    y: torch.Tensor                 # float32 or float64 [sum n]
+    w: Optional[torch.Tensor]       # float32 [sum n] or None (unit weights)
+    periods: torch.Tensor           # float64
+    durations: torch.Tensor         # float64
+    point_offset: np.ndarray        # int64 [n_curves+1]
+    period_begin: np.ndarray        # int64 [n_curves]
+    period_count: np.ndarray        # int64 [n_curves]
+    dur_begin: np.ndarray           # int64 [n_curves]
+    dur_count: np.ndarray           # int32 [n_curves]
+    out_begin: np.ndarray           # int64 [n_curves]
+    time_offset: Optional[np.ndarray] = None
+    _keep: list = field(default_factory=list, repr=False)
+
+    @property
+    def n_curves(self) -> int:
+        return len(self.period_count)
+
+    @property
+    def n_out(self) -> int:
+        return int(np.max(self.out_begin + self.period_count)) if self.n_curves else 0
+
+    @property
+    def device(self) -> torch.device:
+        return self.t.device
+
+    @classmethod
+    def from_arrays(cls, times: Sequence[np.ndarray], fluxes: Sequence[np.ndarray],
+                    flux_errs: Optional[Sequence[Optional[np.ndarray]]] = None,
+                    periods=None, durations=None, device="cuda",
+                    flux_dtype=np.float32, weights=None) -> "CurveBatch":
+        """Pack host arrays into a device batch.
+
+        ``periods``/``durations`` are either one array shared by every curve or a
+        sequence with one array per curve.  Weights are 1/dy^2 rounded to float32
+        (None = unit weights, as gpu_bls.py:63-64); ``weights`` passes per-curve
+        weight arrays directly instead of ``flux_errs``."""
+        nc = len(times)
+        if len(fluxes) != nc:
+            raise ValueError("times and fluxes must have the same number of curves")
+        lens = np.array([len(t) for t in times], dtype=np.int64)
+        for t, y in zip(times, fluxes):
+            if len(t) != len(y):
+                raise ValueError("time and flux must have the same length")
+        pt = np.zeros(nc + 1, np.int64)
+        np.cumsum(lens, out=pt[1:])
+        t_all = np.concatenate([np.asarray(t, np.float64) for t in times]) if nc else np.zeros(0)
+        y_all = np.concatenate([np.asarray(y, flux_dtype) for y in fluxes])
+        w_all = None
+        if weights is not None:
+            ws = [np.asarray(wc, np.float32) for wc in weights]
+            if any(len(wc) != n for wc, n in zip(ws, lens)):
+                raise ValueError("weights and flux must have the same length")
+            w_all = np.concatenate(ws)
+        elif flux_errs is not None and any(e is not None for e in flux_errs):
+            ws = []
+            for e, n in zip(flux_errs, lens):
+                if e is None:
+                    ws.append(np.ones(n, np.float32))
+                else:
+                    e = np.asarray(e, np.float64)
+                    if len(e) != n:
+                        raise ValueError("flux_err and flux must have the same length")
+                    ws.append((1.0 / (e * e)).astype(np.float32))
+            w_all = np.concatenate(ws)
+
+        def grids(g, name):
+            if g is None:
+                raise ValueError(f"{name} must be given")
+            if is_shared_grid(g):
+                arr = np.atleast_1d(np.asarray(g, np.float64))
+                return arr, np.zeros(nc, np.int64), np.full(nc, len(arr), np.int64)
+            if len(g) != nc:
+                raise ValueError(f"{name}: one grid per curve expected")
+            arrs = [np.atleast_1d(np.asarray(a, np.float64)) for a in g]
+            cnt = np.array([len(a) for a in arrs], np.int64)
+            beg = np.zeros(nc, np.int64)
+            np.cumsum(cnt[:-1], out=beg[1:])
+            return np.concatenate(arrs), beg, cnt
+
+        per, pbeg, pcnt = grids(periods, "periods")
+        dur, dbeg, dcnt = grids(durations, "durations")
+        obeg = np.zeros(nc, np.int64)
+        np.cumsum(pcnt[:-1], out=obeg[1:])
+
+        def dev(a):
+            return torch.from_numpy(a).pin_memory().to(device, non_blocking=True)
+
+        return cls(t=dev(t_all), y=dev(y_all), w=None if w_all is None else dev(w_all),
+                   periods=dev(per), durations=dev(dur), point_offset=pt, period_begin=pbeg,
+                   period_count=pcnt, dur_begin=dbeg, dur_count=_i32(dcnt), out_begin=obeg)
+
+
+OUTPUT_FIELDS = ("power", "depth", "depth_err", "t0", "duration", "window")
+_OUT_DTYPES = {"power": torch.float32, "depth": torch.float32, "depth_err": torch.float32,
+               "t0": torch.float64, "duration": torch.float32, "window": torch.int32}
+
+
+def _ptr(x: Optional[torch.Tensor]):
+    return None if x is None else ctypes.c_void_p(x.data_ptr())
+
+
+class SearchPlan:
+    """A batch bound to output tensors; ``execute`` enqueues the search."""
+
+    def __init__(self, engine: "BLSEngine", batch: CurveBatch, config: SearchConfig,
+                 outputs: Dict[str, torch.Tensor]):
+        self.engine = engine
+        self.batch = batch
+        self.config = config
+        self.outputs = outputs
+        lib = engine.handle.lib
+        self._lib = lib
+        # host index arrays must stay alive for the duration of the call only
+        idx = {k: getattr(batch, k) for k in ("point_offset", "period_begin", "period_count",
+                                              "dur_begin", "out_begin")}
+        idx = {k: _i64(v) for k, v in idx.items()}
+        dcnt = _i32(batch.dur_count)
+        toff = None if batch.time_offset is None else _i64(batch.time_offset)
+        b = N.Batch()
+        b.n_curves = batch.n_curves
+        b.y_is_f64 = 1 if batch.y.dtype == torch.float64 else 0
+        b.point_offset = idx["point_offset"].ctypes.data_as(N._i64p)
+        b.time_offset = toff.ctypes.data_as(N._i64p) if toff is not None else None
+        b.period_begin = idx["period_begin"].ctypes.data_as(N._i64p)
+        b.period_count = idx["period_count"].ctypes.data_as(N._i64p)
+        b.dur_begin = idx["dur_begin"].ctypes.data_as(N._i64p)
+        b.dur_count = dcnt.ctypes.data_as(N._i32p)
+        b.out_begin = idx["out_begin"].ctypes.data_as(N._i64p)
+        b.t, b.y, b.w = _ptr(batch.t), _ptr(batch.y), _ptr(batch.w)
+        b.periods, b.durations = _ptr(batch.periods), _ptr(batch.durations)
+        o = N.Outputs()
+        for k in OUTPUT_FIELDS:
+            setattr(o, k, _ptr(outputs.get(k)))
+        o.best_period = _ptr(outputs.get("best_period"))
+        self._params = config.params()
+        ptr = ctypes.c_void_p()
+        with torch.cuda.device(batch.device):
+            rc = lib.atb_plan_create(engine.handle.ptr, ctypes.byref(self._params),
+                                     ctypes.byref(b), ctypes.byref(o), ctypes.byref(ptr))
+        N.raise_for(rc, engine.handle.ptr, "plan creation")
+        self.ptr = ptr
+
+    @property
+    def kernel_count(self) -> int:
+        return int(self._lib.atb_plan_kernel_count(self.ptr))
+
+    @property
+    def scratch_bytes(self) -> int:
+        return int(self._lib.atb_plan_scratch_bytes(self.ptr))
+
+    def execute(self, stream: Optional[torch.cuda.Stream] = None) -> None:
+        s = stream if stream is not None else torch.cuda.current_stream(self.batch.device)
+        rc = self._lib.atb_plan_execute(self.ptr, ctypes.c_void_p(s.cuda_stream))
+        N.raise_for(rc, self.engine.handle.ptr, "plan execution")
+
+    def profile(self, stream: Optional[torch.cuda.Stream] = None) -> Dict[str, float]:
+        """Execute once with CUDA events between the kernels (synchronises);
+        returns milliseconds of the staging, search and best-peak kernels."""
+        s = stream if stream is not None else torch.cuda.current_stream(self.batch.device)
+        ms = [ctypes.c_float(0.0) for _ in range(3)]
+        rc = self._lib.atb_plan_profile(self.ptr, ctypes.c_void_p(s.cuda_stream),
+                                        *(ctypes.byref(m) for m in ms))
+        N.raise_for(rc, self.engine.handle.ptr, "plan profile")
+        return {"stage": ms[0].value, "search": ms[1].value, "best": ms[2].value}
+
+    def check(self) -> None:
+        """Synchronise and raise ValueError if the last execution saw invalid data."""
+        rc = self._lib.atb_plan_check(self.ptr)
+        N.raise_for(rc, self.engine.handle.ptr, "input data")
+
+    def close(self) -> None:
+        if getattr(self, "ptr", None):
+            self._lib.atb_plan_destroy(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class BLSEngine:
+    """Engine bound to one CUDA device."""
+
+    _instances: Dict[int, "BLSEngine"] = {}
+
+    def __init__(self, device=None):
+        if not torch.cuda.is_available():
+            raise RuntimeError("BLSEngine needs a CUDA device (no CPU fallback)")
+        dev = torch.device("cuda", torch.cuda.current_device() if device is None else
+                           torch.device(device).index or 0)
+        self.device = dev
+        self.handle = N.Handle(dev.index)
+
+    @classmethod
+    def get(cls, device=None) -> "BLSEngine":
+        idx = torch.cuda.current_device() if device is None else (torch.device(device).index or 0)
+        eng = cls._instances.get(idx)
+        if eng is None:
+            eng = cls(torch.device("cuda", idx))
+            cls._instances[idx] = eng
+        return eng
+
+    def bench_peaks(self) -> Dict[str, float]:
+        """Measured denominators of the search kernel's roofline on this device:
+        64-bit shared-memory reductions/s (conflict-free and random bins) and
+        FP64 fused multiply-adds/s."""
+        out = {}
+        v = ctypes.c_double(0.0)
+        for name, pat in (("smem_red_u64_per_s", 0), ("smem_red_u64_random_per_s", 1)):
+            rc = self.handle.lib.atb_bench_smem_red_u64(self.handle.ptr, pat, ctypes.byref(v))
+            N.raise_for(rc, self.handle.ptr, "smem benchmark")
+            out[name] = v.value
+        rc = self.handle.lib.atb_bench_dfma(self.handle.ptr, ctypes.byref(v))
+        N.raise_for(rc, self.handle.ptr, "dfma benchmark")
+        out["dfma_per_s"] = v.value
+        return out
+
+    @staticmethod
+    def allocate_outputs(batch: CurveBatch, fields: Sequence[str] = OUTPUT_FIELDS,
+                         best: bool = True) -> Dict[str, torch.Tensor]:
+        n = batch.n_out
+        out = {k: torch.empty(n, dtype=_OUT_DTYPES[k], device=batch.device) for k in fields}
+        if best:
+            out["best_period"] = torch.empty(batch.n_curves, dtype=torch.int32,
+                                             device=batch.device)
+        return out
+
+    def plan(self, batch: CurveBatch, config: SearchConfig,
+             outputs: Optional[Dict[str, torch.Tensor]] = None) -> SearchPlan:
+        if outputs is None:
+            outputs = self.allocate_outputs(batch)
+        return SearchPlan(self, batch, config, outputs)
+
+    def search(self, batch: CurveBatch, config: SearchConfig,
+               stream: Optional[torch.cuda.Stream] = None) -> Dict[str, torch.Tensor]:
+        """Plan, execute, check (synchronises) and return the output tensors."""
+        plan = self.plan(batch, config)
+        try:
+            plan.execute(stream)
+            plan.check()
+            return plan.outputs
+        finally:
+            plan.close()
+
+    def debug_fold(self, t: torch.Tensor, y: torch.Tensor, w: Optional[torch.Tensor],
+                   periods: torch.Tensor, durations: torch.Tensor,
+                   config: SearchConfig) -> torch.Tensor:
+        """Per-point histogram slots [n_periods, n] of one curve (verification)."""
+        n, npd = t.numel(), periods.numel()
+        out = torch.empty((npd, n), dtype=torch.int32, device=t.device)
+        prm = config.params()
+        s = torch.cuda.current_stream(t.device)
+        rc = self.handle.lib.atb_debug_fold(self.handle.ptr, ctypes.byref(prm), _ptr(t), _ptr(y),
+                                            _ptr(w), n, _ptr(periods), npd, _ptr(durations),
+                                            durations.numel(), _ptr(out),
+                                            ctypes.c_void_p(s.cuda_stream))
+        N.raise_for(rc, self.handle.ptr, "debug fold")
+        return out
+
+
+def split_outputs(batch: CurveBatch, outputs: Dict[str, torch.Tensor]) -> List[Dict[str, np.ndarray]]:
+    """Host copies of the outputs, one dict per curve."""
+    host = {k: v.cpu().numpy() for k, v in outputs.items()}
+    res = []
+    for c in range(batch.n_curves):
+        b, n = int(batch.out_begin[c]), int(batch.period_count[c])
+        d = {k: host[k][b:b + n] for k in OUTPUT_FIELDS if k in host}
+        if "best_period" in host:
+            d["best_index"] = int(host["best_period"][c])
+        res.append(d)
+    return res
+
+
+class BatchSession:
+    """A fixed-shape batch kept resident on the device and fed from pinned host
+    memory: the end-to-end path of a batch user.
+
+    The period and duration grids are uploaded once; every :meth:`run` copies
+    the light curves (t float64, y, w float32) from pinned host buffers to the
+    device, executes the plan and copies every per-period output plus the
+    per-curve best index back to pinned host buffers, all on one stream.
+    """
+
+    def __init__(self, engine: BLSEngine, point_offset: np.ndarray, periods, durations,
+                 config: SearchConfig, y_dtype=np.float32, weighted: bool = True,
+                 fields: Sequence[str] = OUTPUT_FIELDS):
+        dev = engine.device
+        pt = _i64(point_offset)
+        n_pts = int(pt[-1])
+        nc = len(pt) - 1
+        tdt = torch.float64 if np.dtype(y_dtype) == np.float64 else torch.float32
+        self.host = {
+            "t": torch.empty(n_pts, dtype=torch.float64).pin_memory(),
+            "y": torch.empty(n_pts, dtype=tdt).pin_memory(),
+        }
+        if weighted:
+            self.host["w"] = torch.empty(n_pts, dtype=torch.float32).pin_memory()
+        self.dev_in = {k: torch.empty_like(v, device=dev) for k, v in self.host.items()}
+        per, pbeg, pcnt = _grid_arrays(periods, nc)
+        dur, dbeg, dcnt = _grid_arrays(durations, nc)
+        obeg = np.zeros(nc, np.int64)
+        np.cumsum(pcnt[:-1], out=obeg[1:])
+        self.batch = CurveBatch(
+            t=self.dev_in["t"], y=self.dev_in["y"], w=self.dev_in.get("w"),
+            periods=torch.from_numpy(per).to(dev), durations=torch.from_numpy(dur).to(dev),
+            point_offset=pt, period_begin=pbeg, period_count=pcnt, dur_begin=dbeg,
+            dur_count=_i32(dcnt), out_begin=obeg)
+        self.outputs = BLSEngine.allocate_outputs(self.batch, fields)
+        self.host_out = {k: torch.empty(v.shape, dtype=v.dtype).pin_memory()
+                         for k, v in self.outputs.items()}
+        self.plan = engine.plan(self.batch, config, self.outputs)
+
+    @property
+    def h2d_bytes(self) -> int:
+        return sum(v.numel() * v.element_size() for v in self.host.values())
+
+    @property
+    def d2h_bytes(self) -> int:
+        return sum(v.numel() * v.element_size() for v in self.host_out.values())
+
+    def load(self, t: np.ndarray, y: np.ndarray, w: Optional[np.ndarray] = None) -> None:
+        """Fill the pinned host input buffers (flattened, curve after curve)."""
+        self.host["t"].numpy()[:] = np.ravel(t)
+        self.host["y"].numpy()[:] = np.ravel(y)
+        if "w" in self.host:
+            self.host["w"].numpy()[:] = np.ravel(w)
+
+    def run(self, stream: Optional[torch.cuda.Stream] = None) -> Dict[str, torch.Tensor]:
+        """Enqueue H2D inputs, the search and D2H outputs on `stream`; the pinned
+        host outputs are valid once the stream has synchronised."""
+        s = stream if stream is not None else torch.cuda.current_stream(self.batch.device)
+        with torch.cuda.stream(s):
+            for k, v in self.host.items():
+                self.dev_in[k].copy_(v, non_blocking=True)
+            self.plan.execute(s)
+            for k, v in self.outputs.items():
+                self.host_out[k].copy_(v, non_blocking=True)
+        return self.host_out
+
+
+def _grid_arrays(g, nc):
+    if is_shared_grid(g):
+        arr = np.atleast_1d(np.asarray(g, np.float64))
+        return arr, np.zeros(nc, np.int64), np.full(nc, len(arr), np.int64)
+    arrs = [np.atleast_1d(np.asarray(a, np.float64)) for a in g]
+    cnt = np.array([len(a) for a in arrs], np.int64)
+    beg = np.zeros(nc, np.int64)
+    np.cumsum(cnt[:-1], out=beg[1:])
+    return np.concatenate(arrs), beg, cnt

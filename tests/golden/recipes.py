@@ -1,0 +1,140 @@
+"""Seeded synthetic light-curve recipes shared by the golden-vector scripts,
+the tests and the benchmark.
+
+The recipes follow the reference test-suite's inputs (``tests/test_v42_parity.py:12-24``,
+``tests/test_astropy_parity.py:15-23``, ``tests/test_synthetic_recovery.py:10-20``)
+and the benchmark workload shapes (single 27.4 d sector with a mid-sector gap,
+box transits injected multiplicatively as ``inject/box.py:21-27`` does).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def inject_box(t, f, period, t0, duration, depth):
+    """Multiplicative box transit, as inject/box.py:3-29 defines it:
+    in transit where |((t - t0 + P/2) mod P) - P/2| < duration/2."""
+    f = np.array(f, dtype=np.float64, copy=True)
+    ph = (t - t0 + 0.5 * period) % period - 0.5 * period
+    f[np.abs(ph) < 0.5 * duration] *= 1.0 - depth
+    return f
+
+
+def v42_test_recipe():
+    """tests/test_v42_parity.py:12-24 (seed 42, 2000 points, dip 0.01 at P=3.521)."""
+    np.random.seed(42)
+    time = np.linspace(0, 27, 2000).astype(np.float64)
+    flux = np.random.normal(0, 0.003, size=2000).astype(np.float64)
+    ph = (time % 3.521) / 3.521
+    flux[ph < (0.1 / 3.521)] -= 0.01
+    flux -= np.mean(flux)
+    dy = np.ones_like(flux) * 0.003
+    periods = np.linspace(3.0, 4.0, 1000).astype(np.float64)
+    durations = np.array([0.05, 0.1, 0.15])
+    return time, flux - np.median(flux), dy, periods, durations
+
+
+def v42_debug_recipe():
+    """tests/debug_v42.py:11-24 (200 points)."""
+    np.random.seed(42)
+    time = np.linspace(0, 27, 200).astype(np.float64)
+    flux = np.random.normal(0, 0.003, size=200).astype(np.float64)
+    ph = (time % 3.521) / 3.521
+    flux[ph < (0.1 / 3.521)] -= 0.01
+    flux -= np.median(flux)
+    dy = np.ones_like(flux) * 0.003
+    return time, flux - np.median(flux), dy, np.linspace(3.0, 4.0, 1000), np.array([0.05, 0.1, 0.15])
+
+
+def astropy_parity_recipe():
+    """tests/test_astropy_parity.py:15-23 (5000 points, P=3.456, fast path n_bins=500)."""
+    np.random.seed(42)
+    t = np.linspace(0, 10, 5000)
+    f = inject_box(t, np.ones_like(t), 3.456, 0.5, 0.1, 0.01)
+    f += np.random.normal(0, 0.001, len(t))
+    return t, f, None, np.linspace(1.0, 5.0, 1000), np.array([0.05, 0.1, 0.15])
+
+
+def recovery_recipe():
+    """tests/test_synthetic_recovery.py:10-20 (P=7.432, t0=1.5, dur 0.15, depth 0.01)."""
+    t = np.linspace(0, 20, 5000)
+    f = inject_box(t, np.ones_like(t), 7.432, 1.5, 0.15, 0.01)
+    np.random.seed(42)
+    f += np.random.normal(0, 0.001, len(t))
+    return t, f, None, np.linspace(5.0, 10.0, 1000), np.linspace(0.05, 0.25, 5)
+
+
+SECTOR_DAYS = 27.4
+C0_DURATIONS = np.array([0.04, 0.06, 0.08, 0.12, 0.16, 0.20])
+
+
+def c0_periods(n=5000, pmin=0.5, pmax=13.7):
+    """Log-spaced period grid of the single-curve workload."""
+    return np.geomspace(pmin, pmax, n)
+
+
+def sector_times(rng, n, t_offset=1325.0, gap=1.0):
+    """n sorted times over one 27.4 d sector with a `gap`-day hole at mid-sector."""
+    out = np.empty(0)
+    lo, hi = 0.5 * (SECTOR_DAYS - gap), 0.5 * (SECTOR_DAYS + gap)
+    while out.size < n:
+        u = SECTOR_DAYS * rng.uniform(size=2 * n)
+        u = u[(u < lo) | (u >= hi)]
+        out = np.concatenate([out, u])
+    return t_offset + np.sort(out[:n])
+
+
+def c0_curve(n=15000, seed=0):
+    """Single-curve workload: N points over a sector with a 1 d mid-sector gap,
+    y = 1 + N(0, 1e-3) with a box transit P=3.71, t0=1326.2, dur=0.10,
+    depth=1.5e-3, dy = 1e-3."""
+    rng = np.random.default_rng(seed)
+    t = sector_times(rng, n)
+    y = 1.0 + rng.normal(0.0, 1e-3, n)
+    y = inject_box(t, y, 3.71, 1326.2, 0.10, 1.5e-3)
+    dy = np.full(n, 1e-3)
+    return t, y, dy
+
+
+CADENCE_2MIN = 2.0 / 1440.0
+
+
+def cadence_grid(t_offset=1325.0, gap=1.0):
+    """2-minute cadence over one sector minus a mid-sector gap."""
+    t = np.arange(0.0, SECTOR_DAYS, CADENCE_2MIN)
+    lo, hi = 0.5 * (SECTOR_DAYS - gap), 0.5 * (SECTOR_DAYS + gap)
+    return t_offset + t[(t < lo) | (t >= hi)]
+
+
+def uniform_batch(n_curves=4096, n=15000, seed=1, transit_fraction=0.3):
+    """Uniform batch: every curve has n float32 points subsampled from the
+    2-minute cadence grid of one sector with a gap, white noise sigma drawn
+    log-uniform in [2e-4, 5e-3], and `transit_fraction` of the curves carry a
+    box transit (P U[0.5,13], dur U[0.03,0.25], depth U[3e-4,1e-2]).
+
+    Returns (t [n_curves, n] float64, y [n_curves, n] float32,
+    dy [n_curves, n] float32, truth list)."""
+    rng = np.random.default_rng(seed)
+    grid = cadence_grid()
+    t = np.empty((n_curves, n), np.float64)
+    y = np.empty((n_curves, n), np.float32)
+    dy = np.empty((n_curves, n), np.float32)
+    truth = []
+    for c in range(n_curves):
+        idx = np.sort(rng.choice(grid.size, size=n, replace=False))
+        tc = grid[idx]
+        sig = float(np.exp(rng.uniform(np.log(2e-4), np.log(5e-3))))
+        yc = 1.0 + rng.normal(0.0, sig, n)
+        tr = None
+        if rng.uniform() < transit_fraction:
+            P = rng.uniform(0.5, 13.0)
+            dur = rng.uniform(0.03, 0.25)
+            dep = rng.uniform(3e-4, 1e-2)
+            t0 = tc[0] + rng.uniform(0.0, P)
+            yc = inject_box(tc, yc, P, t0, dur, dep)
+            tr = (P, t0, dur, dep)
+        t[c] = tc
+        y[c] = yc.astype(np.float32)
+        dy[c] = sig
+        truth.append(tr)
+    return t, y, dy, truth

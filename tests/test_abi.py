@@ -1,0 +1,49 @@
+"""The C-ABI library builds, loads without a GPU and exports every symbol the
+header declares (no compute calls here)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from astro_transit_gpu_b200 import _native as N
+from astro_transit_gpu_b200 import build as B
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include",
+                      "astrotransit_b200.h")
+
+
+def declared_symbols():
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"\b(atb_[a-z_0-9]+)\s*\(", text)))
+
+
+def test_header_and_binding_agree():
+    assert declared_symbols() == sorted(N.EXPORTS)
+
+
+def test_library_loads_and_exports_every_symbol():
+    L = N.load()
+    for name in declared_symbols():
+        assert hasattr(L, name), name
+    assert b"sm_100a" in L.atb_version()
+
+
+def test_library_is_sm100a_only():
+    assert "arch=compute_100a,code=sm_100a" in " ".join(B.NVCC_FLAGS)
+    assert "-fmad=false" in B.NVCC_FLAGS
+
+
+def test_null_handles_are_rejected_without_a_device():
+    L = N.load()
+    assert L.atb_last_error(None, None, 0) == 0
+    assert L.atb_plan_create(None, None, None, None, None) == N.ATB_EINVAL
+    assert L.atb_plan_execute(None, None) == N.ATB_EINVAL
+    assert L.atb_plan_kernel_count(None) == 0
+
+
+def test_structs_match_header_layout():
+    # int32 x6 params; batch: 2 ints + 7 host pointers + 5 device pointers
+    assert ctypes.sizeof(N.Params) == 24
+    assert ctypes.sizeof(N.Batch) == 8 + 12 * 8
+    assert ctypes.sizeof(N.Outputs) == 7 * 8

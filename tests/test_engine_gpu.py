@@ -1,0 +1,297 @@
+"""GPU parity tests: the sm_100a engine against the CPU oracle.
+
+* bit-exact: per-point histogram slots, and every per-period output against the
+  oracle's mirror of the engine arithmetic (oracle.eng_*);
+* tolerance: per-period power within 1e-5 relative of the FP64 restatement of
+  the reference (oracle.ref_*), the same best period, the same winning window
+  wherever the FP64 runner-up trails by more than 1e-5;
+* batching: a ragged batch gives bit-identically what single-curve runs give;
+* edge cases the reference's inputs can reach.
+"""
+import numpy as np
+import pytest
+import torch
+
+import recipes as R
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+POWER_RTOL = 1e-5  # relative power error bound against the FP64 oracle
+FIELDS = ("power", "depth", "depth_err", "t0", "duration", "window")
+
+
+def run(engine, t, y, w, periods, durations, cfg):
+    from astro_transit_gpu_b200.engine import CurveBatch, split_outputs
+    y = np.asarray(y)
+    b = CurveBatch.from_arrays([t], [y], periods=periods, durations=durations,
+                               flux_dtype=np.float64 if y.dtype == np.float64 else np.float32,
+                               weights=None if w is None else [w])
+    return split_outputs(b, engine.search(b, cfg))[0]
+
+
+def cfg_binned(objective="snr", max_bins=None, oversample=10):
+    from astro_transit_gpu_b200.engine import SearchConfig
+    return SearchConfig("parity", objective=objective, max_bins=max_bins, oversample=oversample)
+
+
+def cfg_fixed(n_bins):
+    from astro_transit_gpu_b200.engine import SearchConfig
+    return SearchConfig("fast", n_bins=n_bins)
+
+
+def assert_bit_exact(gpu, ora, name=""):
+    for k in FIELDS:
+        a, b = np.asarray(gpu[k]), np.asarray(ora[k])
+        assert a.dtype == b.dtype, (name, k)
+        bad = np.flatnonzero(a != b)
+        assert bad.size == 0, (name, k, bad[:5], a[bad[:5]], b[bad[:5]])
+
+
+def weighted_unsorted(n=3000, seed=9):
+    rng = np.random.default_rng(seed)
+    t = np.sort(rng.uniform(100.0, 140.0, n))
+    y = R.inject_box(t, 1.0 + rng.normal(0, 1e-3, n), 4.2, 101.0, 0.15, 2e-3)
+    dy = 1e-3 * np.exp(rng.normal(0, 0.5, n))
+    perm = rng.permutation(n)
+    return t[perm], y[perm].astype(np.float32), (1 / dy[perm] ** 2).astype(np.float32)
+
+
+# ------------------------------------------------------------ bit-exact ---
+
+def test_fold_slots_bit_exact(engine):
+    """Per-point bin indices (V42 slots and fixed-bin slots) equal the FP64 fold."""
+    t, y, dy = R.c0_curve(n=5000, seed=1)
+    w = (1 / dy ** 2).astype(np.float32)
+    periods = np.concatenate([R.c0_periods(300), [3.71, 0.5, 13.7, 1.0, 2.0, 4.0]])
+    dev = engine.device
+    tt = torch.tensor(t, device=dev)
+    yy = torch.tensor(y.astype(np.float32), device=dev)
+    ww = torch.tensor(w, device=dev)
+    pp = torch.tensor(periods, device=dev)
+    dd = torch.tensor(R.C0_DURATIONS, device=dev)
+    slots = engine.debug_fold(tt, yy, ww, pp, dd, cfg_binned()).cpu().numpy()
+    ora = O.eng_binned(t, y.astype(np.float32), w, periods, R.C0_DURATIONS, point_bins=True)
+    assert np.array_equal(slots, ora["point_bins"])
+    # counts per bin follow from the indices
+    for p in (0, 150, 305):
+        nb = int(ora["point_bins"][p].max()) + 1
+        assert np.array_equal(np.bincount(slots[p], minlength=nb),
+                              np.bincount(ora["point_bins"][p], minlength=nb))
+    slots = engine.debug_fold(tt, yy, ww, pp, dd, cfg_fixed(200)).cpu().numpy()
+    ora = O.eng_fixed(t, y.astype(np.float32), w, periods, R.C0_DURATIONS, n_bins=200,
+                      point_bins=True)
+    ora_slots = np.where(ora["point_bins"] < 0, 201, ora["point_bins"])
+    assert np.array_equal(slots, ora_slots)
+
+
+@pytest.mark.parametrize("objective", ["snr", "likelihood"])
+def test_binned_bit_exact_reference_recipe(engine, objective):
+    t, y, dy, periods, durs = R.v42_test_recipe()
+    w = (1 / dy ** 2).astype(np.float32)
+    g = run(engine, t, y, w, periods, durs, cfg_binned(objective))
+    o = O.eng_binned(t, y, w, periods, durs, objective=objective)
+    assert_bit_exact(g, o, objective)
+
+
+def test_binned_bit_exact_c0_float32(engine):
+    t, y, dy = R.c0_curve(n=15000, seed=0)
+    y32 = y.astype(np.float32)
+    w = (1 / dy ** 2).astype(np.float32)
+    periods = R.c0_periods(1000)
+    g = run(engine, t, y32, w, periods, R.C0_DURATIONS, cfg_binned("likelihood"))
+    o = O.eng_binned(t, y32, w, periods, R.C0_DURATIONS, objective="likelihood")
+    assert_bit_exact(g, o, "c0")
+
+
+def test_binned_bit_exact_weighted_unsorted(engine):
+    t, y, w = weighted_unsorted()
+    periods, durs = np.geomspace(0.7, 15.0, 700), np.array([0.05, 0.1, 0.2, 0.3])
+    g = run(engine, t, y, w, periods, durs, cfg_binned())
+    o = O.eng_binned(t, y, w, periods, durs)
+    assert_bit_exact(g, o, "weighted")
+
+
+def test_binned_bit_exact_reference_cap(engine):
+    t, y, dy = R.c0_curve(n=3000, seed=7)
+    w = (1 / dy ** 2).astype(np.float32)
+    periods = R.c0_periods(400)
+    g = run(engine, t, y, w, periods, R.C0_DURATIONS, cfg_binned(max_bins=2000))
+    o = O.eng_binned(t, y, w, periods, R.C0_DURATIONS, max_bins=2000)
+    assert_bit_exact(g, o, "cap")
+
+
+def test_binned_global_histogram_fallback(engine):
+    """Periods whose bin count exceeds shared memory use the global-memory
+    histograms; results stay bit-exact (here up to ~60k bins)."""
+    rng = np.random.default_rng(4)
+    t = np.sort(rng.uniform(0, 60.0, 4000))
+    y = R.inject_box(t, 1.0 + rng.normal(0, 1e-3, t.size), 11.0, 3.0, 0.05, 3e-3)
+    w = np.full(t.size, 1e6, np.float32)
+    periods = np.array([2.0, 5.0, 11.0, 12.0])
+    durs = np.array([0.002, 0.02, 0.05])
+    g = run(engine, t, y, w, periods, durs, cfg_binned())
+    o = O.eng_binned(t, y, w, periods, durs)
+    assert_bit_exact(g, o, "fallback")
+
+
+@pytest.mark.parametrize("n_bins", [200, 500, 1024, 3000])
+def test_fixed_bit_exact(engine, n_bins):
+    t, f, _, periods, durs = R.astropy_parity_recipe()
+    g = run(engine, t, f, None, periods, durs, cfg_fixed(n_bins))
+    o = O.eng_fixed(t, f, None, periods, durs, n_bins=n_bins)
+    assert_bit_exact(g, o, f"fixed{n_bins}")
+
+
+def test_fixed_bit_exact_weighted_unsorted(engine):
+    t, y, w = weighted_unsorted(n=2000, seed=3)
+    periods, durs = np.linspace(1.0, 6.0, 500), np.array([0.05, 0.1, 0.2])
+    g = run(engine, t, y, w, periods, durs, cfg_fixed(300))
+    o = O.eng_fixed(t, y, w, periods, durs, n_bins=300)
+    assert_bit_exact(g, o, "fixed-weighted")
+
+
+# ------------------------------------------------ tolerance vs FP64 ref ---
+
+def test_power_within_tolerance_of_fp64_reference(engine):
+    t, y, dy = R.c0_curve(n=15000, seed=0)
+    periods = R.c0_periods(2000)
+    w64 = 1 / dy ** 2
+    for objective in ("snr", "likelihood"):
+        g = run(engine, t, y, w64.astype(np.float32), periods, R.C0_DURATIONS,
+                cfg_binned(objective))
+        a = O.ref_binned(t, y, w64, periods, R.C0_DURATIONS, objective=objective)
+        rel = np.abs(g["power"] - a["power"]) / a["power"]
+        assert rel.max() <= POWER_RTOL, rel.max()
+        assert np.argmax(g["power"]) == np.argmax(a["power"])
+        ok = a["gap"] > 1e-5
+        assert np.array_equal(g["window"][ok], a["window"][ok])
+        assert np.max(np.abs(g["t0"][ok] - a["t0"][ok])) < 1e-9
+        assert np.max(np.abs(g["depth"][ok] - a["depth"][ok]) / np.abs(a["depth"][ok])) < 1e-5
+    # the injected transit is the best peak
+    assert abs(periods[np.argmax(g["power"])] - 3.71) < 0.01
+
+
+def test_fast_power_within_tolerance_of_fp64_reference(engine):
+    t, f, _, periods, durs = R.astropy_parity_recipe()
+    g = run(engine, t, f, None, periods, durs, cfg_fixed(500))
+    a = O.ref_fixed(t, f, None, periods, durs, n_bins=500)
+    rel = np.abs(g["power"] - a["power"]) / a["power"]
+    assert rel.max() <= POWER_RTOL
+    assert np.argmax(g["power"]) == np.argmax(a["power"])
+
+
+# ------------------------------------------------------------- batching ---
+
+def test_ragged_batch_equals_single_curve_runs(engine):
+    from astro_transit_gpu_b200.engine import CurveBatch, split_outputs
+    rng = np.random.default_rng(21)
+    ts, ys, ws, ps, ds = [], [], [], [], []
+    for k, n in enumerate([37, 1000, 5003, 12000, 1]):
+        t = np.sort(rng.uniform(0, 27.4, n)) + 1300.0 + k
+        y = (1.0 + rng.normal(0, 1e-3, n)).astype(np.float32)
+        ts.append(t); ys.append(y)
+        ws.append(np.full(n, 1e6 * (k + 1), np.float32))
+        ps.append(np.geomspace(0.5, 13.7, 100 + 97 * k))
+        ds.append(np.array([0.04, 0.08, 0.16])[: 1 + k % 3])
+    b = CurveBatch.from_arrays(ts, ys, periods=ps, durations=ds, weights=ws)
+    outs = split_outputs(b, engine.search(b, cfg_binned()))
+    for k in range(len(ts)):
+        single = run(engine, ts[k], ys[k], ws[k], ps[k], ds[k], cfg_binned())
+        assert_bit_exact(outs[k], single, f"curve{k}")
+        o = O.eng_binned(ts[k], ys[k], ws[k], ps[k], ds[k])
+        assert_bit_exact(outs[k], o, f"oracle{k}")
+        assert outs[k]["best_index"] == int(np.argmax(single["power"]))
+
+
+def test_results_are_bit_deterministic(engine):
+    t, y, dy = R.c0_curve(n=8000, seed=4)
+    w = (1 / dy ** 2).astype(np.float32)
+    periods = R.c0_periods(1500)
+    a = run(engine, t, y, w, periods, R.C0_DURATIONS, cfg_binned())
+    b = run(engine, t, y, w, periods, R.C0_DURATIONS, cfg_binned())
+    assert_bit_exact(a, b, "rerun")
+
+
+# -------------------------------------------------------------- edge cases ---
+
+def test_edge_cases(engine):
+    # one point: no window has points both in and out of transit
+    g = run(engine, np.array([1.0]), np.array([1.0], np.float32), None, [1.0, 2.0], [0.1],
+            cfg_binned())
+    assert np.all(g["power"] == 0) and np.all(g["window"] == -1)
+    # constant flux: zero depth everywhere, identical to the oracle
+    t = np.linspace(0, 10, 500)
+    y = np.ones(500, np.float32)
+    g = run(engine, t, y, None, np.linspace(1, 3, 50), [0.1, 0.2], cfg_binned())
+    o = O.eng_binned(t, y, None, np.linspace(1, 3, 50), [0.1, 0.2])
+    assert_bit_exact(g, o, "flat")
+    assert np.all(g["power"] == 0)
+    # durations longer than some periods, single period, float64 flux
+    t, f, _, _, _ = R.recovery_recipe()
+    g = run(engine, t, f, None, [0.3], [0.05, 0.25, 0.5], cfg_binned())
+    o = O.eng_binned(t, f, None, [0.3], [0.05, 0.25, 0.5])
+    assert_bit_exact(g, o, "long-durations")
+
+
+# -------------------------------------------------------- drop-in API ---
+
+def test_api_synthetic_recovery():
+    """tests/test_synthetic_recovery.py: best period within 0.01 of the truth."""
+    from astro_transit_gpu_b200 import run_gpu_bls
+    t, f, _, periods, durs = R.recovery_recipe()
+    res = run_gpu_bls(t, f, periods, durs)
+    assert abs(res["best_period"] - 7.432) < 0.01
+
+
+def test_api_v42_parity_recipe():
+    """tests/test_v42_parity.py's assertions, against the FP64 restatement
+    (Astropy itself is not available): corr > 0.99999, max |diff| < 1e-4."""
+    from astro_transit_gpu_b200 import BoxLeastSquaresGPU
+    t, y, dy, periods, durs = R.v42_test_recipe()
+    res = BoxLeastSquaresGPU(t, y, dy).power(periods, durs, method="parity", dtype=np.float64,
+                                             max_bins=4000)
+    a = O.ref_binned(t, y, 1 / dy ** 2, periods, durs, max_bins=4000)
+    assert np.corrcoef(a["power"], res.power)[0, 1] > 0.99999
+    assert np.max(np.abs(a["power"] - res.power)) < 1e-4
+    assert res.power.dtype == np.float64
+    assert abs(res.best_period - 3.521) < 0.01
+    assert len(res.top_candidates) == 5
+    assert res.depth is not None and res.transit_time is not None
+
+
+def test_api_fast_astropy_recipe():
+    """tests/test_astropy_parity.py's best-period and top-1 checks."""
+    from astro_transit_gpu_b200 import BoxLeastSquaresGPU
+    t, f, _, periods, durs = R.astropy_parity_recipe()
+    res = BoxLeastSquaresGPU(t, f).power(periods, durs, n_bins=500, dtype=np.float32)
+    assert abs(res.best_period - 3.456) < 0.01
+    assert abs(res.top_candidates[0].period - 3.456) < 0.01
+    a = O.ref_fixed(t, f, None, periods, durs, n_bins=500)
+    assert np.corrcoef(a["power"], res.power)[0, 1] > 0.9999
+
+
+def test_api_grid_consistency():
+    """tests/test_cpu_gpu_grid_consistency.py: best period and depth of the box."""
+    from astro_transit_gpu_b200 import run_gpu_bls
+    t = np.linspace(0, 10, 5000)
+    f = R.inject_box(t, np.ones_like(t), 3.456, 1.2, 0.1, 0.01)
+    f += np.random.default_rng(0).normal(0, 1e-4, len(t))
+    res = run_gpu_bls(t, f, np.linspace(2.0, 5.0, 500), np.linspace(0.05, 0.15, 3))
+    assert abs(res["best_period"] - 3.456) < 0.01
+    assert abs(res["best_depth"] - 0.01) < 0.005
+
+
+def test_api_multi_target_parity():
+    from astro_transit_gpu_b200 import run_vbls_exact_parity
+    rng = np.random.default_rng(5)
+    t = np.linspace(0.0, 20.0, 1200)
+    ys = np.stack([R.inject_box(t, 1.0 + rng.normal(0, 1e-3, t.size), 2.0 + k, 0.3 * k, 0.1, 3e-3)
+                   for k in range(3)])
+    ws = (1.0 / (1e-3 * (1.0 + rng.uniform(size=ys.shape))) ** 2)
+    periods, durs = np.linspace(1.5, 5.0, 300), np.array([0.06, 0.1, 0.14])
+    r = run_vbls_exact_parity(t, ys, periods, durs, weights_matrix=ws, max_bins=2000)
+    for k in range(3):
+        o = O.eng_binned(t, ys[k], ws[k].astype(np.float32), periods, durs, max_bins=2000)
+        assert np.array_equal(r["power_array"][k], o["power"])
+        assert abs(r["best_period"][k] - (2.0 + k)) < 0.02
