@@ -47,10 +47,18 @@ constexpr int kR = 8;                  // consecutive points a thread holds in r
 constexpr int kTileP = 64;             // periods per work-queue tile
 constexpr int kMaxG = 64;              // periods per shared-memory group
 constexpr int kMaxDur = 32;            // durations per curve
-constexpr int kQBits = 26;             // |q| <= 2^kQBits per point
 constexpr int kStageAlign = 32;        // staged curves start at multiples of 32 points
 constexpr int kStageBlock = 256;
+constexpr double kMagicRound = 4503599627370496.0;  // 2^52: x + 2^52 (rz) truncates x in [0, 2^31)
+constexpr double kMagicFloor = 6755399441055744.0;  // 1.5*2^52: (m + C)(rd) - C = floor(m), |m| < 2^50
 
+// Per-curve fixed-point layout.  Point values are quantised to |q| <= 2^qbits;
+// histogram words hold the low `lobits` bits and the arithmetic-shifted high
+// part of each value in separate 32-bit counters, sized so neither can
+// overflow for the curve's point count n (bitlen = bits of n):
+//   low sums  < n * 2^lobits            <= 2^32
+//   high sums < n * 2^(qbits - lobits)  <= 2^31
+// with lobits = 32 - bitlen and qbits = min(26, 63 - 2*bitlen).
 struct CurveStat {
     double t_start;
     double shift;
@@ -61,8 +69,14 @@ struct CurveStat {
     int s_y;
     double bin_dur;      // BINNED: min(duration) / oversample
     double inv_bin_dur;  // BINNED: 1 / bin_dur
+    double dt_absmax;    // max |t - t_start|
     int n_dur;
-    int pad;
+    int qbits;
+    int lobits;
+    int qw0;        // the common q_w when uniform_w
+    int uniform_w;  // every q_w equal: the weight words count points
+    int thr_unit;   // 1e-15 (the reference's empty-window threshold) is below one
+                    // quantised weight unit: "W < 1e-15" is then "W == 0"
 };
 
 struct StageArgs {
@@ -124,11 +138,26 @@ struct SearchArgs {
 // shared device helpers
 // ----------------------------------------------------------------------------
 
-__device__ __forceinline__ int q_scale(double m) {
+__device__ __forceinline__ int q_scale(double m, int qbits) {
     if (!(m > 0.0)) return 0;
     int e;
     frexp(m, &e);
-    return kQBits - e;
+    return qbits - e;
+}
+
+__device__ __forceinline__ int bitlen64(long long n) { return n <= 0 ? 0 : 64 - __clzll(n); }
+__device__ __forceinline__ int curve_lobits(long long n) { return min(30, 32 - bitlen64(n)); }
+__device__ __forceinline__ int curve_qbits(long long n) { return min(26, 63 - 2 * bitlen64(n)); }
+
+// floor(m) for |m| < 2^50 with two full-rate FP64 additions (exact)
+__device__ __forceinline__ double floor_magic(double m) {
+    return __dadd_rn(__dadd_rd(m, kMagicFloor), -kMagicFloor);
+}
+
+// trunc(x) for x in (-1, 2^31) as an int, with one full-rate FP64 addition;
+// x in (-1, 0) yields a negative value (callers clamp at 0, as int(x) = 0 there)
+__device__ __forceinline__ int trunc_magic(double x) {
+    return __double2loint(__dadd_rz(x, kMagicRound));
 }
 
 __device__ __forceinline__ double ll_as_d(long long v) { return __longlong_as_double(v); }
@@ -141,28 +170,6 @@ __device__ __forceinline__ int binned_nbins(double period, double inv_bin_dur, i
     int nb = (int)x + oversample;
     if (max_bins > 0 && nb >= max_bins) nb = max_bins - 1;
     return nb;
-}
-
-// astropy-binned fold: ph = t - P*floor(t/P) (fused), ind = int(ph/bin_dur)+1
-// (vbls_v42_parity.cu:65-70); returns the histogram slot in [0, nb].
-__device__ __forceinline__ int fold_binned(double d, double period, double inv_period,
-                                           double inv_bin_dur, int nb) {
-    const double m = d * inv_period;
-    const double ph = fma(-period, floor(m), d);
-    const double x = ph * inv_bin_dur;
-    int ind = __double2int_rz(x) + 1;
-    ind = min(ind, nb);
-    ind = max(ind, 0);
-    return ind;
-}
-
-// fixed-bin fold: phase = frac(t_rel*inv_p), bin = int(phase*n_bins) (bls.cu:52-62);
-// returns bin+1, or the trash slot nb+1 for points the reference drops.
-__device__ __forceinline__ int fold_fixed(double d, double inv_p, double nbd, int nb) {
-    const double m = d * inv_p;
-    const double ph = m - floor(m);
-    const int b = __double2int_rz(ph * nbd);
-    return (b >= 0 && b < nb) ? b + 1 : nb + 1;
 }
 
 // Exact comparison of candidates a = an/ad and b = bn/bd (floats, positive
@@ -260,9 +267,11 @@ __global__ void __launch_bounds__(kStageBlock) stage_kernel(const StageArgs a) {
     const float* w = a.w ? a.w + p0 : nullptr;
     const long long so = a.stage_off[c];
     const long long n_pad = (n + kR - 1) / kR * kR;
+    const int qbits = curve_qbits(n);
+    const double t_start = n > 0 ? t[0] : 0.0;
 
     // pass 1: magnitudes and validity
-    double wmax = 0.0, amax = 0.0;
+    double wmax = 0.0, amax = 0.0, tmax = 0.0;
     int bad = 0;
     for (long long i = threadIdx.x; i < n; i += kStageBlock) {
         const double wi = w ? (double)w[i] : 1.0;
@@ -270,12 +279,14 @@ __global__ void __launch_bounds__(kStageBlock) stage_kernel(const StageArgs a) {
         if (!(wi > 0.0) || !isfinite(wi) || !isfinite(yi) || !isfinite(t[i])) bad = 1;
         wmax = max(wmax, wi);
         amax = max(amax, fabs(wi * yi));
+        tmax = max(tmax, fabs(t[i] - t_start));
     }
     wmax = block_max_d(wmax, shd);
     amax = block_max_d(amax, shd);
+    tmax = block_max_d(tmax, shd);
     if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(a.status, 1);
-    const int s_w = q_scale(wmax);
-    const int s_a = q_scale(amax);
+    const int s_w = q_scale(wmax, qbits);
+    const int s_a = q_scale(amax, qbits);
 
     // pass 2: exact integer sums -> the shift c (weighted mean of y)
     long long sqw = 0, sqa = 0;
@@ -296,11 +307,11 @@ __global__ void __launch_bounds__(kStageBlock) stage_kernel(const StageArgs a) {
         vmax = max(vmax, fabs(wi * ((double)y[i] - shift)));
     }
     vmax = block_max_d(vmax, shd);
-    const int s_y = q_scale(vmax);
+    const int s_y = q_scale(vmax, qbits);
 
     // pass 4: staged arrays (padded with zero-weight points) and totals
-    const double t_start = n > 0 ? t[0] : 0.0;
     long long qw_tot = 0, qy_tot = 0, qy_abs = 0;
+    int qw_min = 0x7fffffff, qw_max = -1;
     for (long long i = threadIdx.x; i < n_pad; i += kStageBlock) {
         double d = 0.0;
         int qa = 0, qb = 0;
@@ -309,6 +320,8 @@ __global__ void __launch_bounds__(kStageBlock) stage_kernel(const StageArgs a) {
             qa = (int)__double2ll_rn(ldexp(wi, s_w));
             qb = (int)__double2ll_rn(ldexp(wi * ((double)y[i] - shift), s_y));
             d = t[i] - t_start;
+            qw_min = min(qw_min, qa);
+            qw_max = max(qw_max, qa);
         }
         a.sdt[so + i] = d;
         a.sqw[so + i] = qa;
@@ -320,6 +333,8 @@ __global__ void __launch_bounds__(kStageBlock) stage_kernel(const StageArgs a) {
     qw_tot = block_sum_ll(qw_tot, shl);
     qy_tot = block_sum_ll(qy_tot, shl);
     qy_abs = block_sum_ll(qy_abs, shl);
+    qw_max = (int)block_max_d((double)qw_max, shd);
+    qw_min = -(int)block_max_d(-(double)qw_min, shd);
 
     if (threadIdx.x == 0) {
         const int nd = a.dur_cnt[c];
@@ -340,8 +355,13 @@ __global__ void __launch_bounds__(kStageBlock) stage_kernel(const StageArgs a) {
         st.s_y = s_y;
         st.bin_dur = bin_dur;
         st.inv_bin_dur = ibd;
+        st.dt_absmax = tmax;
         st.n_dur = nd;
-        st.pad = 0;
+        st.qbits = qbits;
+        st.lobits = curve_lobits(n);
+        st.uniform_w = (n > 0 && qw_min == qw_max) ? 1 : 0;
+        st.qw0 = n > 0 ? qw_max : 0;
+        st.thr_unit = ldexp(1e-15, s_w) < 1.0 ? 1 : 0;
         a.stats[c] = st;
     }
 }
@@ -350,17 +370,60 @@ __global__ void __launch_bounds__(kStageBlock) stage_kernel(const StageArgs a) {
 // search kernel
 // ----------------------------------------------------------------------------
 
-template <bool GLOB>
-__device__ __forceinline__ void hist_add(longlong2* H, int slot, int aw, int ay) {
+__device__ __forceinline__ void red_shared_u32(unsigned addr, unsigned v) {
+    asm volatile("red.shared.add.u32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
+}
+
+// Histogram entry of slot s: four 32-bit words -- weight sums split at
+// `lobits` (x, y; x = point count when weights are uniform) and flux sums
+// split the same way (z, w).  Component c is stored in word c ^ rot(s),
+// rot(s) = (s >> 3) & 3, so that for a fixed component consecutive slots
+// cycle through all 32 banks (a plain 16-byte layout would use only 8).
+__device__ __forceinline__ unsigned slot_rot(int s) { return ((unsigned)s >> 3) & 3u; }
+
+__device__ __forceinline__ uint4 load_components(const uint4* H, int s) {
+    uint4 e = H[s];
+    const unsigned r = slot_rot(s);
+    if (r & 1u) {
+        const unsigned t0 = e.x, t1 = e.z;
+        e.x = e.y; e.y = t0; e.z = e.w; e.w = t1;
+    }
+    if (r & 2u) {
+        const unsigned t0 = e.x, t1 = e.y;
+        e.x = e.z; e.y = e.w; e.z = t0; e.w = t1;
+    }
+    return e;
+}
+
+__device__ __forceinline__ void store_components(uint4* H, int s, uint4 e) {
+    const unsigned r = slot_rot(s);  // the rotation is an involution per bit
+    if (r & 1u) {
+        const unsigned t0 = e.x, t1 = e.z;
+        e.x = e.y; e.y = t0; e.z = e.w; e.w = t1;
+    }
+    if (r & 2u) {
+        const unsigned t0 = e.x, t1 = e.y;
+        e.x = e.z; e.y = e.w; e.z = t0; e.w = t1;
+    }
+    H[s] = e;
+}
+
+template <bool GLOB, bool UNI>
+__device__ __forceinline__ void hist_add(uint4* H, int slot, unsigned dwl, unsigned dwh, unsigned dyl,
+                                         unsigned dyh) {
+    const unsigned r = slot_rot(slot);
     if (GLOB) {
-        atomicAdd(reinterpret_cast<unsigned long long*>(&H[slot].x),
-                  (unsigned long long)(long long)aw);
-        atomicAdd(reinterpret_cast<unsigned long long*>(&H[slot].y),
-                  (unsigned long long)(long long)ay);
+        unsigned* e = reinterpret_cast<unsigned*>(H + slot);
+        atomicAdd(e + (0u ^ r), dwl);
+        if (!UNI) atomicAdd(e + (1u ^ r), dwh);
+        atomicAdd(e + (2u ^ r), dyl);
+        atomicAdd(e + (3u ^ r), dyh);
     } else {
-        const unsigned addr = (unsigned)__cvta_generic_to_shared(&H[slot]);
-        asm volatile("red.shared.add.u64 [%0], %1;" ::"r"(addr), "l"((long long)aw) : "memory");
-        asm volatile("red.shared.add.u64 [%0+8], %1;" ::"r"(addr), "l"((long long)ay) : "memory");
+        const unsigned b = (unsigned)__cvta_generic_to_shared(H + slot) | (r << 2);
+        red_shared_u32(b, dwl);
+        if (!UNI) red_shared_u32(b ^ 4u, dwh);
+        red_shared_u32(b ^ 8u, dyl);
+        red_shared_u32(b ^ 12u, dyh);
     }
 }
 
@@ -381,6 +444,8 @@ __device__ __forceinline__ void team_sync(const Team& tm) {
 }
 
 struct GroupSmem {
+    double tP[kTileP];   // the tile's periods
+    int tNB[kTileP];     // and their bin counts
     double P[kMaxG];
     double IP[kMaxG];
     int NB[kMaxG];
@@ -399,19 +464,69 @@ struct GroupSmem {
     int G;
     int total;
     int glob;
+    int safe_floor;  // |dt / P| < 2^50 over the group: floor via floor_magic
 };
 
+// Histogram slots of one thread's kR points for one period.
+//   astropy-binned (vbls_v42_parity.cu:65-70): ph = fma(-P, floor(d*IP), d),
+//     slot = min(int(ph*inv_bin_dur) + 1, n_bins)
+//   fixed bins (bls.cu:52-62): ph = d*IP - floor(d*IP), b = int(ph*n_bins),
+//     slot = b + 1, or the trash slot n_bins + 1 for b outside [0, n_bins)
+// floor and trunc are computed with exact
+// magic-constant additions, and when the points are time-ordered and the first
+// and last share the cycle index k = floor(d*IP), every point between them has
+// the same k (rounded multiplication and floor are monotone), so k is reused.
 template <int GEOM>
-__device__ __forceinline__ int fold_slot(double d, double P, double IP, double k_bins, int NB) {
-    if (GEOM == ATB_GEOM_BINNED) return fold_binned(d, P, IP, k_bins, NB);
-    return fold_fixed(d, IP, k_bins, NB);
+__device__ __forceinline__ void fold_slots(const double (&d)[kR], bool sorted, bool safe_floor,
+                                           double P, double IP, double ibd, int NB, int (&sl)[kR]) {
+    double k0, k7;
+    const double m0 = d[0] * IP, m7 = d[kR - 1] * IP;
+    if (safe_floor) {
+        k0 = floor_magic(m0);
+        k7 = floor_magic(m7);
+    } else {
+        k0 = floor(m0);
+        k7 = floor(m7);
+    }
+    const double nbd = (double)NB;
+    if (sorted && k0 == k7) {
+#pragma unroll
+        for (int j = 0; j < kR; ++j) {
+            if (GEOM == ATB_GEOM_BINNED) {
+                const double ph = fma(-P, k0, d[j]);
+                const int ind = max(trunc_magic(ph * ibd), 0) + 1;
+                sl[j] = min(ind, NB);
+            } else {
+                const double m = (j == 0) ? m0 : (j == kR - 1 ? m7 : d[j] * IP);
+                const int b = trunc_magic((m - k0) * nbd);
+                sl[j] = (b < NB) ? b + 1 : NB + 1;
+            }
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < kR; ++j) {
+            const double m = d[j] * IP;
+            const double k = safe_floor ? floor_magic(m) : floor(m);
+            if (GEOM == ATB_GEOM_BINNED) {
+                const double ph = fma(-P, k, d[j]);
+                const int ind = max(trunc_magic(ph * ibd), 0) + 1;
+                sl[j] = min(ind, NB);
+            } else {
+                const int b = trunc_magic((m - k) * nbd);
+                sl[j] = (b >= 0 && b < NB) ? b + 1 : NB + 1;
+            }
+        }
+    }
 }
 
 // fold every staged point of the curve into the group's histograms
-template <int GEOM, bool GLOB>
-__device__ void fold_group(const SearchArgs& a, const GroupSmem& gs, longlong2* H, long long so,
-                           long long n_pad, double k_bins_binned) {
+template <int GEOM, bool GLOB, bool UNI>
+__device__ void fold_group(const SearchArgs& a, const GroupSmem& gs, uint4* H, long long so,
+                           long long n_pad, const CurveStat& st) {
     const int G = gs.G;
+    const bool safe = gs.safe_floor != 0;
+    const int L = st.lobits;
+    const unsigned lomask = (1u << L) - 1u;
     for (long long base = 0; base < n_pad; base += (long long)kBlock * kR) {
         const long long i0 = base + (long long)threadIdx.x * kR;
         if (i0 >= n_pad) continue;
@@ -433,27 +548,39 @@ __device__ void fold_group(const SearchArgs& a, const GroupSmem& gs, longlong2* 
             qw[4 * q] = vw.x; qw[4 * q + 1] = vw.y; qw[4 * q + 2] = vw.z; qw[4 * q + 3] = vw.w;
             qy[4 * q] = vy.x; qy[4 * q + 1] = vy.y; qy[4 * q + 2] = vy.z; qy[4 * q + 3] = vy.w;
         }
-        for (int g = 0; g < G; ++g) {
-            const double P = gs.P[g];
-            const double IP = gs.IP[g];
-            const int NB = gs.NB[g];
-            const double kb = (GEOM == ATB_GEOM_BINNED) ? k_bins_binned : (double)NB;
-            longlong2* Hg = H + gs.base[g];
-            int cur = fold_slot<GEOM>(d[0], P, IP, kb, NB);
-            int aw = qw[0], ay = qy[0];
+        bool sorted = true;
 #pragma unroll
-            for (int j = 1; j < kR; ++j) {
-                const int s = fold_slot<GEOM>(d[j], P, IP, kb, NB);
-                if (s != cur) {
-                    hist_add<GLOB>(Hg, cur, aw, ay);
-                    cur = s;
-                    aw = 0;
-                    ay = 0;
+        for (int j = 0; j + 1 < kR; ++j) sorted = sorted && (d[j] <= d[j + 1]);
+        // running sums of the split words over the thread's points
+        unsigned pwl[kR], pwh[kR], pyl[kR], pyh[kR];
+        {
+            unsigned aw = 0, bw = 0, ay = 0, by = 0;
+#pragma unroll
+            for (int j = 0; j < kR; ++j) {
+                if (UNI) {
+                    aw += qw[j] != 0 ? 1u : 0u;  // padding points carry q_w = 0
+                } else {
+                    aw += (unsigned)qw[j] & lomask;
+                    bw += (unsigned)(qw[j] >> L);
                 }
-                aw += qw[j];
-                ay += qy[j];
+                ay += (unsigned)qy[j] & lomask;
+                by += (unsigned)(qy[j] >> L);
+                pwl[j] = aw; pwh[j] = bw; pyl[j] = ay; pyh[j] = by;
             }
-            hist_add<GLOB>(Hg, cur, aw, ay);
+        }
+        for (int g = 0; g < G; ++g) {
+            const int NB = gs.NB[g];
+            int sl[kR];
+            fold_slots<GEOM>(d, sorted, safe, gs.P[g], gs.IP[g], st.inv_bin_dur, NB, sl);
+            uint4* Hg = H + gs.base[g];
+            unsigned lw = 0, lh = 0, ly = 0, lz = 0;
+#pragma unroll
+            for (int j = 0; j < kR; ++j) {
+                if (j == kR - 1 || sl[j] != sl[j + 1]) {
+                    hist_add<GLOB, UNI>(Hg, sl[j], pwl[j] - lw, pwh[j] - lh, pyl[j] - ly, pyh[j] - lz);
+                    lw = pwl[j]; lh = pwh[j]; ly = pyl[j]; lz = pyh[j];
+                }
+            }
         }
     }
 }
@@ -482,16 +609,32 @@ __device__ void window_stats(double dw, double dy, double wtot, double ytot, int
     *derr = de;
 }
 
-// exclusive->inclusive scan of H[0..M) in place, int64 -> exact FP64 bit patterns
-__device__ void team_scan(const Team& tm, GroupSmem& gs, longlong2* E, int M) {
-    const int seg = (M + tm.nthreads - 1) / tm.nthreads;
+// Inclusive scan of the raw histogram entries H[0..M) in place: each entry's
+// split 32-bit words are combined into exact int64 sums (W, Y) and the
+// running sums are written back as exact FP64 values (|sum| < 2^53).
+// Threads own contiguous segments of odd length, so the 16-byte entries a
+// warp touches in one step fall in distinct bank groups.
+__device__ __forceinline__ void entry_sums(const uint4 e, int L, bool uni, long long qw0,
+                                           long long& w, long long& y) {
+    w = uni ? (long long)e.x * qw0 : (long long)e.y * (1LL << L) + (long long)e.x;
+    y = (long long)(int)e.w * (1LL << L) + (long long)e.z;
+}
+
+__device__ void team_scan(const Team& tm, GroupSmem& gs, longlong2* E, int M, const CurveStat& st) {
+    int seg = (M + tm.nthreads - 1) / tm.nthreads;
+    seg |= 1;
     const int b = min(M, tm.tid * seg);
     const int e = min(M, b + seg);
+    const int L = st.lobits;
+    const bool uni = st.uniform_w != 0;
+    const long long qw0 = st.qw0;
+    const uint4* R = reinterpret_cast<const uint4*>(E);
     long long sw = 0, sy = 0;
     for (int i = b; i < e; ++i) {
-        const longlong2 v = E[i];
-        sw += v.x;
-        sy += v.y;
+        long long w, y;
+        entry_sums(load_components(R, i), L, uni, qw0, w, y);
+        sw += w;
+        sy += y;
     }
     const int lane = threadIdx.x & 31;
     long long iw = sw, iy = sy;
@@ -519,9 +662,10 @@ __device__ void team_scan(const Team& tm, GroupSmem& gs, longlong2* E, int M) {
     }
     long long xw = iw - sw, xy = iy - sy;
     for (int i = b; i < e; ++i) {
-        const longlong2 v = E[i];
-        xw += v.x;
-        xy += v.y;
+        long long w, y;
+        entry_sums(load_components(R, i), L, uni, qw0, w, y);
+        xw += w;
+        xy += y;
         E[i] = make_longlong2(__double_as_longlong((double)xw), __double_as_longlong((double)xy));
     }
     team_sync(tm);
@@ -553,6 +697,117 @@ __device__ Cand team_best(const Team& tm, GroupSmem& gs, Cand c) {
     return c;
 }
 
+struct WinConsts {
+    double wtot, ytot;  // exact totals (quantised units)
+    float invw;         // 1 / W
+    float ks;           // 1 / sum|q_y|
+    float stot;         // S * ks
+    double thr;         // 1e-15 in quantised weight units
+};
+
+// One (start, duration) window from exact FP64 prefix values: returns false
+// when the window is skipped, else its FP32 score numerator and denominator.
+//   BINNED (vbls_v42_parity.cu:103-116): skip empty in/out windows, dip-only
+//   FIXED  (bls.cu:128): skip unless 0 < W_in < W
+template <int GEOM, bool UNIT>
+__device__ __forceinline__ bool window_eval(double dw, double dy, const WinConsts& kc, float& num,
+                                            float& den) {
+    const double wo = kc.wtot - dw;
+    const float fdw = __double2float_rn(dw);
+    const float fwo = __double2float_rn(wo);
+    bool ok;
+    if (UNIT) {
+        ok = fdw > 0.0f && fwo > 0.0f;  // exact: dw, wo are integers and thr < 1
+    } else {
+        ok = !(dw < kc.thr || wo < kc.thr);
+    }
+    const float u = __fmul_rn(fdw, kc.invw);
+    const float v = __fmul_rn(fwo, kc.invw);
+    const float av = __fmul_rn(__double2float_rn(dy), kc.ks);
+    const float sig = __fmaf_rn(kc.stot, u, -av);
+    if (GEOM == ATB_GEOM_BINNED) ok = ok && (sig >= 0.0f);
+    num = __fmul_rn(sig, sig);
+    den = __fmul_rn(u, v);
+    return ok;
+}
+
+// All windows of one period over starts tid, tid+nthreads, ...  NDMAX > 0:
+// up to NDMAX durations unrolled, every end point loaded before evaluation.
+template <int GEOM, int NDMAX, bool UNIT>
+__device__ Cand window_search(const longlong2* E, int NB, int nd, const int* lens_smem, int tid,
+                              int nthreads, const WinConsts& kc) {
+    Cand best{-1.0f, 1.0f, 0x7fffffff};
+    if (NDMAX > 0) {
+        int len[NDMAX > 0 ? NDMAX : 1];
+#pragma unroll
+        for (int k = 0; k < NDMAX; ++k) len[k] = k < nd ? lens_smem[k] : (1 << 29);
+        for (int s = tid; s < NB; s += nthreads) {
+            const longlong2 e0 = E[s];
+            const double c0w = ll_as_d(e0.x), c0y = ll_as_d(e0.y);
+            longlong2 e1[NDMAX > 0 ? NDMAX : 1];
+#pragma unroll
+            for (int k = 0; k < NDMAX; ++k) {
+                int idx = s + len[k];
+                if (GEOM == ATB_GEOM_FIXED && idx > NB) idx -= NB;
+                e1[k] = E[min(idx, NB)];
+            }
+#pragma unroll
+            for (int k = 0; k < NDMAX; ++k) {
+                if (k >= nd) break;
+                double dw, dy;
+                bool in_range;
+                if (GEOM == ATB_GEOM_BINNED) {
+                    in_range = s + len[k] <= NB;
+                    dw = ll_as_d(e1[k].x) - c0w;
+                    dy = ll_as_d(e1[k].y) - c0y;
+                } else {
+                    in_range = len[k] < NB;
+                    if (s + len[k] <= NB) {
+                        dw = ll_as_d(e1[k].x) - c0w;
+                        dy = ll_as_d(e1[k].y) - c0y;
+                    } else {
+                        dw = (kc.wtot - c0w) + ll_as_d(e1[k].x);
+                        dy = (kc.ytot - c0y) + ll_as_d(e1[k].y);
+                    }
+                }
+                float num, den;
+                const bool ok = window_eval<GEOM, UNIT>(dw, dy, kc, num, den);
+                if (in_range && ok) cand_consider(best, num, den, s * nd + k);
+            }
+        }
+    } else {
+        for (int s = tid; s < NB; s += nthreads) {
+            const longlong2 e0 = E[s];
+            const double c0w = ll_as_d(e0.x), c0y = ll_as_d(e0.y);
+            for (int k = 0; k < nd; ++k) {
+                const int L = lens_smem[k];
+                double dw, dy;
+                if (GEOM == ATB_GEOM_BINNED) {
+                    if (s + L > NB) continue;
+                    const longlong2 e1 = E[s + L];
+                    dw = ll_as_d(e1.x) - c0w;
+                    dy = ll_as_d(e1.y) - c0y;
+                } else {
+                    if (L >= NB) continue;
+                    if (s + L <= NB) {
+                        const longlong2 e1 = E[s + L];
+                        dw = ll_as_d(e1.x) - c0w;
+                        dy = ll_as_d(e1.y) - c0y;
+                    } else {
+                        const longlong2 e1 = E[s + L - NB];
+                        dw = (kc.wtot - c0w) + ll_as_d(e1.x);
+                        dy = (kc.ytot - c0y) + ll_as_d(e1.y);
+                    }
+                }
+                float num, den;
+                if (window_eval<GEOM, UNIT>(dw, dy, kc, num, den))
+                    cand_consider(best, num, den, s * nd + k);
+            }
+        }
+    }
+    return best;
+}
+
 template <int GEOM>
 __device__ void finalize_period(const SearchArgs& a, GroupSmem& gs, const Team& tm, longlong2* H,
                                 int g, const CurveStat& st, int nd) {
@@ -564,7 +819,9 @@ __device__ void finalize_period(const SearchArgs& a, GroupSmem& gs, const Team& 
     if (GEOM == ATB_GEOM_BINNED) {
         // padding copy, vbls_v42_parity.cu:78-80 (sequential semantics)
         if (tm.tid == 0) {
-            for (int j = 1, ind = NB - a.oversample; j <= a.oversample; ++j, ++ind) E[ind] = E[j];
+            uint4* R = reinterpret_cast<uint4*>(E);
+            for (int j = 1, ind = NB - a.oversample; j <= a.oversample; ++j, ++ind)
+                store_components(R, ind, load_components(R, j));
         }
         team_sync(tm);
     } else {
@@ -574,7 +831,7 @@ __device__ void finalize_period(const SearchArgs& a, GroupSmem& gs, const Team& 
             gs.L[tm.id][tm.tid] = L;
         }
     }
-    team_scan(tm, gs, E, NB + 1);
+    team_scan(tm, gs, E, NB + 1, st);
 
     const double ay = st.qy_abs > 0 ? (double)st.qy_abs : 1.0;
     const float ks = (float)(1.0 / ay);
@@ -589,54 +846,24 @@ __device__ void finalize_period(const SearchArgs& a, GroupSmem& gs, const Team& 
     }
     Cand best{-1.0f, 1.0f, 0x7fffffff};
     if (wtot > 0.0) {
-        const float invw = (float)(1.0 / wtot);
-        const float stot = (float)(ytot / ay);
-        if (GEOM == ATB_GEOM_BINNED) {
-            const double thr = ldexp(1e-15, st.s_w);
-            for (int s = tm.tid; s < NB; s += tm.nthreads) {
-                const longlong2 e0 = E[s];
-                const double c0w = ll_as_d(e0.x), c0y = ll_as_d(e0.y);
-                for (int k = 0; k < nd; ++k) {
-                    const int dd = gs.dbins[k];
-                    if (s + dd > NB) continue;
-                    const longlong2 e1 = E[s + dd];
-                    const double dw = ll_as_d(e1.x) - c0w;
-                    const double dy = ll_as_d(e1.y) - c0y;
-                    const double wo = wtot - dw;
-                    if (dw < thr || wo < thr) continue;
-                    const float u = __fmul_rn(__double2float_rn(dw), invw);
-                    const float v = __fmul_rn(__double2float_rn(wo), invw);
-                    const float av = __fmul_rn(__double2float_rn(dy), ks);
-                    const float sig = __fmaf_rn(stot, u, -av);
-                    if (!(sig >= 0.0f)) continue;
-                    cand_consider(best, __fmul_rn(sig, sig), __fmul_rn(u, v), s * nd + k);
-                }
-            }
+        WinConsts kc;
+        kc.wtot = wtot;
+        kc.ytot = ytot;
+        kc.invw = (float)(1.0 / wtot);
+        kc.ks = ks;
+        kc.stot = (float)(ytot / ay);
+        kc.thr = ldexp(1e-15, st.s_w);
+        const int* lens = (GEOM == ATB_GEOM_BINNED) ? gs.dbins : gs.L[tm.id];
+        const bool unit = GEOM == ATB_GEOM_FIXED || st.thr_unit;
+        if (nd <= 4) {
+            best = unit ? window_search<GEOM, 4, true>(E, NB, nd, lens, tm.tid, tm.nthreads, kc)
+                        : window_search<GEOM, 4, false>(E, NB, nd, lens, tm.tid, tm.nthreads, kc);
+        } else if (nd <= 8) {
+            best = unit ? window_search<GEOM, 8, true>(E, NB, nd, lens, tm.tid, tm.nthreads, kc)
+                        : window_search<GEOM, 8, false>(E, NB, nd, lens, tm.tid, tm.nthreads, kc);
         } else {
-            for (int s = tm.tid; s < NB; s += tm.nthreads) {
-                const longlong2 e0 = E[s];
-                const double c0w = ll_as_d(e0.x), c0y = ll_as_d(e0.y);
-                for (int k = 0; k < nd; ++k) {
-                    const int L = gs.L[tm.id][k];
-                    if (L >= NB) continue;
-                    double dw, dy;
-                    if (s + L <= NB) {
-                        const longlong2 e1 = E[s + L];
-                        dw = ll_as_d(e1.x) - c0w;
-                        dy = ll_as_d(e1.y) - c0y;
-                    } else {
-                        const longlong2 e1 = E[s + L - NB];
-                        dw = (wtot - c0w) + ll_as_d(e1.x);
-                        dy = (ytot - c0y) + ll_as_d(e1.y);
-                    }
-                    if (!(dw > 0.0 && dw < wtot)) continue;
-                    const float u = __fmul_rn(__double2float_rn(dw), invw);
-                    const float v = __fmul_rn(__double2float_rn(wtot - dw), invw);
-                    const float av = __fmul_rn(__double2float_rn(dy), ks);
-                    const float sig = __fmaf_rn(stot, u, -av);
-                    cand_consider(best, __fmul_rn(sig, sig), __fmul_rn(u, v), s * nd + k);
-                }
-            }
+            best = unit ? window_search<GEOM, 0, true>(E, NB, nd, lens, tm.tid, tm.nthreads, kc)
+                        : window_search<GEOM, 0, false>(E, NB, nd, lens, tm.tid, tm.nthreads, kc);
         }
     }
     best = team_best(tm, gs, best);
@@ -691,7 +918,11 @@ __device__ void run_group(const SearchArgs& a, GroupSmem& gs, longlong2* H, cons
     const int total = gs.total;
     for (int i = threadIdx.x; i < total; i += kBlock) H[i] = make_longlong2(0, 0);
     __syncthreads();
-    fold_group<GEOM, GLOB>(a, gs, H, so, n_pad, st.inv_bin_dur);
+    uint4* HU = reinterpret_cast<uint4*>(H);
+    if (st.uniform_w)
+        fold_group<GEOM, GLOB, true>(a, gs, HU, so, n_pad, st);
+    else
+        fold_group<GEOM, GLOB, false>(a, gs, HU, so, n_pad, st);
     __syncthreads();
     const int G = gs.G;
     int tw = 1;
@@ -746,23 +977,33 @@ __global__ void __launch_bounds__(kBlock, 1) search_kernel(const SearchArgs a) {
         }
         long long pn = gs.pb;
         const long long pe = gs.pe;
+        // the tile's periods and bin counts, loaded in parallel
+        for (int i = threadIdx.x; i < (int)(pe - pn); i += kBlock) {
+            double P = a.periods[pbeg + pn + i];
+            if (!(P > 0.0) || !(P < 1.0e300)) {
+                atomicOr(a.status, 4);
+                P = 1.0;
+            }
+            gs.tP[i] = P;
+            gs.tNB[i] = (GEOM == ATB_GEOM_BINNED)
+                            ? binned_nbins(P, st.inv_bin_dur, a.oversample, a.max_bins)
+                            : a.n_bins_fixed;
+        }
+        __syncthreads();
         while (pn < pe) {
             if (threadIdx.x == 0) {
                 int g = 0, base = 0;
                 long long p = pn;
+                double ipmax = 0.0;
                 while (p < pe && g < kMaxG) {
-                    double P = a.periods[pbeg + p];
-                    if (!(P > 0.0) || !(P < 1.0e300)) {
-                        atomicOr(a.status, 4);
-                        P = 1.0;
-                    }
-                    const int NB = (GEOM == ATB_GEOM_BINNED)
-                                       ? binned_nbins(P, st.inv_bin_dur, a.oversample, a.max_bins)
-                                       : a.n_bins_fixed;
+                    const int li = (int)(p - gs.pb);
+                    const double P = gs.tP[li];
+                    const int NB = gs.tNB[li];
                     const int need = NB + 2;
                     if (g > 0 && base + need > a.cap) break;
                     gs.P[g] = P;
                     gs.IP[g] = 1.0 / P;
+                    ipmax = max(ipmax, gs.IP[g]);
                     gs.NB[g] = NB;
                     gs.base[g] = base;
                     gs.slot[g] = obeg + p;
@@ -774,6 +1015,7 @@ __global__ void __launch_bounds__(kBlock, 1) search_kernel(const SearchArgs a) {
                 gs.G = g;
                 gs.total = base;
                 gs.glob = base > a.cap ? 1 : 0;
+                gs.safe_floor = (st.dt_absmax * ipmax < 1.0e15) ? 1 : 0;
             }
             __syncthreads();
             if (gs.glob) {
@@ -811,22 +1053,35 @@ __global__ void best_kernel(int n_curves, const long long* per_cnt, const long l
     if (lane == 0) best[warp] = cnt > 0 ? (int)bi : -1;
 }
 
-// per-point histogram slots of curve 0 for every period (verification only)
+// per-point histogram slots of curve 0 for every period (verification only):
+// the same staged points, chunking and fold_slots code as the search kernel
 template <int GEOM>
 __global__ void debug_fold_kernel(const double* sdt, long long n, const CurveStat* stats,
                                   const double* periods, long long n_periods, int oversample,
                                   int max_bins, int n_bins_fixed, int* out) {
-    const long long total = n * n_periods;
+    const long long n_pad = (n + kR - 1) / kR * kR;
+    const long long chunks = n_pad / kR;
     const CurveStat st = stats[0];
-    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < chunks * n_periods;
          idx += (long long)gridDim.x * blockDim.x) {
-        const long long p = idx / n, i = idx % n;
+        const long long p = idx / chunks, ch = idx % chunks;
         const double P = periods[p];
         const int NB = (GEOM == ATB_GEOM_BINNED)
                            ? binned_nbins(P, st.inv_bin_dur, oversample, max_bins)
                            : n_bins_fixed;
-        const double kb = (GEOM == ATB_GEOM_BINNED) ? st.inv_bin_dur : (double)NB;
-        out[idx] = fold_slot<GEOM>(sdt[i], P, 1.0 / P, kb, NB);
+        double d[kR];
+        bool sorted = true;
+#pragma unroll
+        for (int j = 0; j < kR; ++j) d[j] = sdt[ch * kR + j];
+#pragma unroll
+        for (int j = 0; j + 1 < kR; ++j) sorted = sorted && (d[j] <= d[j + 1]);
+        const double IP = 1.0 / P;
+        const bool safe = st.dt_absmax * IP < 1.0e15;
+        int sl[kR];
+        fold_slots<GEOM>(d, sorted, safe, P, IP, st.inv_bin_dur, NB, sl);
+#pragma unroll
+        for (int j = 0; j < kR; ++j)
+            if (ch * kR + j < n) out[p * n + ch * kR + j] = sl[j];
     }
 }
 

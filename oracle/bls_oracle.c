@@ -339,7 +339,15 @@ int orc_ref_fixed(int64_t n, const double* t, const double* y, const double* w, 
 /* (B) the engine's exact arithmetic                                          */
 /* ------------------------------------------------------------------------- */
 
-#define ENG_QBITS 26 /* per-point fixed-point magnitude bound: |q| <= 2^26 */
+/* Per-point fixed-point magnitude bound |q| <= 2^qbits with
+ * qbits = min(26, 63 - 2*bitlen(n)), bitlen(n) = number of bits of the point
+ * count n: the engine's 32-bit split histogram words cannot overflow. */
+static int eng_qbits(int64_t n)
+{
+    const int bl = n > 0 ? 64 - __builtin_clzll((unsigned long long)n) : 0;
+    const int b = 63 - 2 * bl;
+    return b < 26 ? b : 26;
+}
 
 typedef struct {
     double t_start;
@@ -351,13 +359,13 @@ typedef struct {
     int32_t s_y;
 } orc_stage_stats;
 
-/* Scale exponent s such that m * 2^s <= 2^ENG_QBITS for m = max |value|. */
-static int q_scale(double m)
+/* Scale exponent s such that m * 2^s <= 2^qbits for m = max |value|. */
+static int q_scale(double m, int qbits)
 {
     if (!(m > 0.0)) return 0;
     int e;
     frexp(m, &e); /* m = f * 2^e, f in [0.5, 1) so m < 2^e */
-    return ENG_QBITS - e;
+    return qbits - e;
 }
 
 /*
@@ -381,8 +389,9 @@ int orc_eng_stage(int64_t n, const double* t, const double* y, const float* w, d
         const double a = fabs(wi * y[i]);
         if (a > amax) amax = a;
     }
-    const int s_w = q_scale(wmax);
-    const int s_a = q_scale(amax);
+    const int qbits = eng_qbits(n);
+    const int s_w = q_scale(wmax, qbits);
+    const int s_a = q_scale(amax, qbits);
     int64_t sum_qw = 0, sum_qa = 0;
     for (int64_t i = 0; i < n; ++i) {
         const double wi = w ? (double)w[i] : 1.0;
@@ -396,7 +405,7 @@ int orc_eng_stage(int64_t n, const double* t, const double* y, const float* w, d
         const double v = fabs(wi * (y[i] - shift));
         if (v > vmax) vmax = v;
     }
-    const int s_y = q_scale(vmax);
+    const int s_y = q_scale(vmax, qbits);
     int64_t qw_tot = 0, qy_tot = 0, qy_abs = 0;
     const double t_start = t[0];
     for (int64_t i = 0; i < n; ++i) {

@@ -104,6 +104,22 @@ def test_binned_bit_exact_c0_float32(engine):
     assert_bit_exact(g, o, "c0")
 
 
+@pytest.mark.parametrize("n", [1, 7, 9, 4095, 5003])
+def test_binned_bit_exact_odd_lengths(engine, n):
+    """Curves whose length is not a multiple of the per-thread chunk (padding)."""
+    rng = np.random.default_rng(n)
+    t = np.sort(rng.uniform(0, 27.4, n)) + 1300.0
+    y = (1.0 + rng.normal(0, 1e-3, n)).astype(np.float32)
+    periods, durs = np.geomspace(0.5, 13.7, 300), np.array([0.04, 0.08, 0.16])
+    for w in (None, np.full(n, 4e5, np.float32), rng.uniform(1e5, 1e6, n).astype(np.float32)):
+        g = run(engine, t, y, w, periods, durs, cfg_binned())
+        o = O.eng_binned(t, y, w, periods, durs)
+        assert_bit_exact(g, o, f"n={n}")
+        g = run(engine, t, y, w, periods, durs, cfg_fixed(200))
+        o = O.eng_fixed(t, y, w, periods, durs, n_bins=200)
+        assert_bit_exact(g, o, f"fixed n={n}")
+
+
 def test_binned_bit_exact_weighted_unsorted(engine):
     t, y, w = weighted_unsorted()
     periods, durs = np.geomspace(0.7, 15.0, 700), np.array([0.05, 0.1, 0.2, 0.3])
