@@ -41,9 +41,23 @@
 
 namespace {
 
-constexpr int kBlock = 512;            // threads of a search CTA
-constexpr int kWarps = kBlock / 32;    // 16
-constexpr int kR = 8;                  // consecutive points a thread holds in registers
+#ifndef ATB_BLOCK
+#define ATB_BLOCK 512
+#endif
+#ifndef ATB_MIN_BLOCKS
+#define ATB_MIN_BLOCKS 2
+#endif
+#ifndef ATB_POINTS_PER_THREAD
+#define ATB_POINTS_PER_THREAD 4
+#endif
+constexpr int kBlock = ATB_BLOCK;            // threads of a search CTA
+constexpr int kMinBlocks = ATB_MIN_BLOCKS;   // resident search CTAs per SM
+constexpr int kWarps = kBlock / 32;
+// Teams of tw warps (tw a power of two) must tile the CTA exactly, so that
+// every warp of a team reaches the team's named barrier.
+static_assert(kBlock % 32 == 0 && kWarps >= 2 && kWarps <= 32 && (kWarps & (kWarps - 1)) == 0,
+              "search CTA: a power-of-two number of warps, at most 1024 threads");
+constexpr int kR = ATB_POINTS_PER_THREAD;    // consecutive points a thread holds in registers
 constexpr int kTileP = 64;             // periods per work-queue tile
 constexpr int kMaxG = 64;              // periods per shared-memory group
 constexpr int kMaxDur = 32;            // durations per curve
@@ -77,6 +91,9 @@ struct CurveStat {
     int uniform_w;  // every q_w equal: the weight words count points
     int thr_unit;   // 1e-15 (the reference's empty-window threshold) is below one
                     // quantised weight unit: "W < 1e-15" is then "W == 0"
+    int ew;         // prefix sums are stored as exact FP64 values scaled by 2^-ew (weights)
+    int ey;         // and 2^-ey (flux), so that |W| < 1 and |S| <= 1
+    int pad2;
 };
 
 struct StageArgs {
@@ -190,14 +207,6 @@ struct Cand {
     float num, den;
     int key;
 };
-
-__device__ __forceinline__ void cand_consider(Cand& b, float num, float den, int key) {
-    if (cand_better(num, den, key, b.num, b.den, b.key)) {
-        b.num = num;
-        b.den = den;
-        b.key = key;
-    }
-}
 
 __device__ __forceinline__ Cand warp_best(Cand c) {
 #pragma unroll
@@ -362,6 +371,12 @@ __global__ void __launch_bounds__(kStageBlock) stage_kernel(const StageArgs a) {
         st.uniform_w = (n > 0 && qw_min == qw_max) ? 1 : 0;
         st.qw0 = n > 0 ? qw_max : 0;
         st.thr_unit = ldexp(1e-15, s_w) < 1.0 ? 1 : 0;
+        int ew = 0, ey = 0;
+        if (qw_tot > 0) frexp((double)qw_tot, &ew);
+        if (qy_abs > 0) frexp((double)qy_abs, &ey);
+        st.ew = ew;
+        st.ey = ey;
+        st.pad2 = 0;
         a.stats[c] = st;
     }
 }
@@ -574,6 +589,7 @@ __device__ void fold_group(const SearchArgs& a, const GroupSmem& gs, uint4* H, l
             fold_slots<GEOM>(d, sorted, safe, gs.P[g], gs.IP[g], st.inv_bin_dur, NB, sl);
             uint4* Hg = H + gs.base[g];
             unsigned lw = 0, lh = 0, ly = 0, lz = 0;
+            // runs of equal slots are merged: one reduction per run, at its end
 #pragma unroll
             for (int j = 0; j < kR; ++j) {
                 if (j == kR - 1 || sl[j] != sl[j + 1]) {
@@ -585,7 +601,8 @@ __device__ void fold_group(const SearchArgs& a, const GroupSmem& gs, uint4* H, l
     }
 }
 
-// FP64 statistics of the winning window (exact quantised sums)
+// FP64 statistics of the winning window from exact scaled sums: real units
+// are W = dw * 2^-s_w, S = dy * 2^-s_y (s_w, s_y net of the prefix scaling)
 __device__ void window_stats(double dw, double dy, double wtot, double ytot, int s_w, int s_y,
                              int objective, double* power, double* depth, double* derr) {
     const double w_in = ldexp(dw, -s_w);
@@ -611,7 +628,8 @@ __device__ void window_stats(double dw, double dy, double wtot, double ytot, int
 
 // Inclusive scan of the raw histogram entries H[0..M) in place: each entry's
 // split 32-bit words are combined into exact int64 sums (W, Y) and the
-// running sums are written back as exact FP64 values (|sum| < 2^53).
+// running sums are written back as exact FP64 values scaled by 2^-ew, 2^-ey
+// (|sum| < 2^53, so both the conversion and the scaling are exact).
 // Threads own contiguous segments of odd length, so the 16-byte entries a
 // warp touches in one step fall in distinct bank groups.
 __device__ __forceinline__ void entry_sums(const uint4 e, int L, bool uni, long long qw0,
@@ -661,12 +679,14 @@ __device__ void team_scan(const Team& tm, GroupSmem& gs, longlong2* E, int M, co
         iy += oy;
     }
     long long xw = iw - sw, xy = iy - sy;
+    const double sw2 = ldexp(1.0, -st.ew), sy2 = ldexp(1.0, -st.ey);
     for (int i = b; i < e; ++i) {
         long long w, y;
         entry_sums(load_components(R, i), L, uni, qw0, w, y);
         xw += w;
         xy += y;
-        E[i] = make_longlong2(__double_as_longlong((double)xw), __double_as_longlong((double)xy));
+        E[i] = make_longlong2(__double_as_longlong((double)xw * sw2),
+                              __double_as_longlong((double)xy * sy2));
     }
     team_sync(tm);
 }
@@ -698,15 +718,16 @@ __device__ Cand team_best(const Team& tm, GroupSmem& gs, Cand c) {
 }
 
 struct WinConsts {
-    double wtot, ytot;  // exact totals (quantised units)
-    float invw;         // 1 / W
-    float ks;           // 1 / sum|q_y|
-    float stot;         // S * ks
-    double thr;         // 1e-15 in quantised weight units
+    double wtot, ytot;  // exact totals, scaled like the prefix sums
+    float c1;           // ytot / wtot
+    double thr;         // 1e-15 in scaled weight units
 };
 
-// One (start, duration) window from exact FP64 prefix values: returns false
-// when the window is skipped, else its FP32 score numerator and denominator.
+// One (start, duration) window from exact scaled FP64 prefix values: returns
+// false when the window is skipped, else FP32 num/den of a score proportional
+// to the objective within the period:
+//   sigma = (S/W) W_in - S_in,  num = sigma^2,  den = W_in W_out
+//   (num/den = depth^2 W_in W_out / W^2, the SNR^2 up to a per-period factor)
 //   BINNED (vbls_v42_parity.cu:103-116): skip empty in/out windows, dip-only
 //   FIXED  (bls.cu:128): skip unless 0 < W_in < W
 template <int GEOM, bool UNIT>
@@ -717,43 +738,63 @@ __device__ __forceinline__ bool window_eval(double dw, double dy, const WinConst
     const float fwo = __double2float_rn(wo);
     bool ok;
     if (UNIT) {
-        ok = fdw > 0.0f && fwo > 0.0f;  // exact: dw, wo are integers and thr < 1
+        ok = fdw > 0.0f && fwo > 0.0f;  // exact: dw, wo are scaled integers and thr < 1 unit
     } else {
         ok = !(dw < kc.thr || wo < kc.thr);
     }
-    const float u = __fmul_rn(fdw, kc.invw);
-    const float v = __fmul_rn(fwo, kc.invw);
-    const float av = __fmul_rn(__double2float_rn(dy), kc.ks);
-    const float sig = __fmaf_rn(kc.stot, u, -av);
+    const float sig = __fmaf_rn(kc.c1, fdw, -__double2float_rn(dy));
     if (GEOM == ATB_GEOM_BINNED) ok = ok && (sig >= 0.0f);
     num = __fmul_rn(sig, sig);
-    den = __fmul_rn(u, v);
+    den = __fmul_rn(fdw, fwo);
     return ok;
 }
 
-// All windows of one period over starts tid, tid+nthreads, ...  NDMAX > 0:
-// up to NDMAX durations unrolled, every end point loaded before evaluation.
-template <int GEOM, int NDMAX, bool UNIT>
+// Running best with a division-free pre-filter: `lim` is a lower bound of the
+// best ratio (rounded down by 2^-20), so num < lim*den can never win the exact
+// comparison and skips it.
+struct Best {
+    Cand c;
+    float lim;
+    __device__ __forceinline__ void init() {
+        c = Cand{-1.0f, 1.0f, 0x7fffffff};
+        lim = -2.0f;
+    }
+    __device__ __forceinline__ void consider(float num, float den, int key) {
+        if (num >= __fmul_rn(lim, den) && cand_better(num, den, key, c.num, c.den, c.key)) {
+            c.num = num;
+            c.den = den;
+            c.key = key;
+            lim = __fmul_rn(__fdiv_rn(num, den), 0.99999904632568359375f);  // 1 - 2^-20
+        }
+    }
+};
+
+// All windows of one period over starts tid, tid+nthreads, ...  Durations are
+// taken four at a time: the four end points are loaded before any is used
+// (instruction-level parallelism with few live registers).
+template <int GEOM, bool UNIT>
 __device__ Cand window_search(const longlong2* E, int NB, int nd, const int* lens_smem, int tid,
                               int nthreads, const WinConsts& kc) {
-    Cand best{-1.0f, 1.0f, 0x7fffffff};
-    if (NDMAX > 0) {
-        int len[NDMAX > 0 ? NDMAX : 1];
+    constexpr int kC = 4;
+    Best best;
+    best.init();
+    for (int k0 = 0; k0 < nd; k0 += kC) {
+        int len[kC];
 #pragma unroll
-        for (int k = 0; k < NDMAX; ++k) len[k] = k < nd ? lens_smem[k] : (1 << 29);
+        for (int k = 0; k < kC; ++k) len[k] = k0 + k < nd ? lens_smem[k0 + k] : (1 << 29);
         for (int s = tid; s < NB; s += nthreads) {
             const longlong2 e0 = E[s];
             const double c0w = ll_as_d(e0.x), c0y = ll_as_d(e0.y);
-            longlong2 e1[NDMAX > 0 ? NDMAX : 1];
+            longlong2 e1[kC];
 #pragma unroll
-            for (int k = 0; k < NDMAX; ++k) {
+            for (int k = 0; k < kC; ++k) {
                 int idx = s + len[k];
                 if (GEOM == ATB_GEOM_FIXED && idx > NB) idx -= NB;
                 e1[k] = E[min(idx, NB)];
             }
 #pragma unroll
-            for (int k = 0; k < NDMAX; ++k) {
-                if (k >= nd) break;
+            for (int k = 0; k < kC; ++k) {
+                if (k0 + k >= nd) break;  // uniform across the team
                 double dw, dy;
                 bool in_range;
                 if (GEOM == ATB_GEOM_BINNED) {
@@ -772,40 +813,11 @@ __device__ Cand window_search(const longlong2* E, int NB, int nd, const int* len
                 }
                 float num, den;
                 const bool ok = window_eval<GEOM, UNIT>(dw, dy, kc, num, den);
-                if (in_range && ok) cand_consider(best, num, den, s * nd + k);
-            }
-        }
-    } else {
-        for (int s = tid; s < NB; s += nthreads) {
-            const longlong2 e0 = E[s];
-            const double c0w = ll_as_d(e0.x), c0y = ll_as_d(e0.y);
-            for (int k = 0; k < nd; ++k) {
-                const int L = lens_smem[k];
-                double dw, dy;
-                if (GEOM == ATB_GEOM_BINNED) {
-                    if (s + L > NB) continue;
-                    const longlong2 e1 = E[s + L];
-                    dw = ll_as_d(e1.x) - c0w;
-                    dy = ll_as_d(e1.y) - c0y;
-                } else {
-                    if (L >= NB) continue;
-                    if (s + L <= NB) {
-                        const longlong2 e1 = E[s + L];
-                        dw = ll_as_d(e1.x) - c0w;
-                        dy = ll_as_d(e1.y) - c0y;
-                    } else {
-                        const longlong2 e1 = E[s + L - NB];
-                        dw = (kc.wtot - c0w) + ll_as_d(e1.x);
-                        dy = (kc.ytot - c0y) + ll_as_d(e1.y);
-                    }
-                }
-                float num, den;
-                if (window_eval<GEOM, UNIT>(dw, dy, kc, num, den))
-                    cand_consider(best, num, den, s * nd + k);
+                if (in_range && ok) best.consider(num, den, s * nd + k0 + k);
             }
         }
     }
-    return best;
+    return best.c;
 }
 
 template <int GEOM>
@@ -833,12 +845,10 @@ __device__ void finalize_period(const SearchArgs& a, GroupSmem& gs, const Team& 
     }
     team_scan(tm, gs, E, NB + 1, st);
 
-    const double ay = st.qy_abs > 0 ? (double)st.qy_abs : 1.0;
-    const float ks = (float)(1.0 / ay);
-    double wtot, ytot;
+    double wtot, ytot;  // scaled exact totals
     if (GEOM == ATB_GEOM_BINNED) {
-        wtot = (double)st.qw_tot;
-        ytot = (double)st.qy_tot;
+        wtot = ldexp((double)st.qw_tot, -st.ew);
+        ytot = ldexp((double)st.qy_tot, -st.ey);
     } else {
         const longlong2 te = E[NB];
         wtot = ll_as_d(te.x);
@@ -849,22 +859,12 @@ __device__ void finalize_period(const SearchArgs& a, GroupSmem& gs, const Team& 
         WinConsts kc;
         kc.wtot = wtot;
         kc.ytot = ytot;
-        kc.invw = (float)(1.0 / wtot);
-        kc.ks = ks;
-        kc.stot = (float)(ytot / ay);
-        kc.thr = ldexp(1e-15, st.s_w);
+        kc.c1 = (float)(ytot / wtot);
+        kc.thr = ldexp(1e-15, st.s_w - st.ew);
         const int* lens = (GEOM == ATB_GEOM_BINNED) ? gs.dbins : gs.L[tm.id];
         const bool unit = GEOM == ATB_GEOM_FIXED || st.thr_unit;
-        if (nd <= 4) {
-            best = unit ? window_search<GEOM, 4, true>(E, NB, nd, lens, tm.tid, tm.nthreads, kc)
-                        : window_search<GEOM, 4, false>(E, NB, nd, lens, tm.tid, tm.nthreads, kc);
-        } else if (nd <= 8) {
-            best = unit ? window_search<GEOM, 8, true>(E, NB, nd, lens, tm.tid, tm.nthreads, kc)
-                        : window_search<GEOM, 8, false>(E, NB, nd, lens, tm.tid, tm.nthreads, kc);
-        } else {
-            best = unit ? window_search<GEOM, 0, true>(E, NB, nd, lens, tm.tid, tm.nthreads, kc)
-                        : window_search<GEOM, 0, false>(E, NB, nd, lens, tm.tid, tm.nthreads, kc);
-        }
+        best = unit ? window_search<GEOM, true>(E, NB, nd, lens, tm.tid, tm.nthreads, kc)
+                    : window_search<GEOM, false>(E, NB, nd, lens, tm.tid, tm.nthreads, kc);
     }
     best = team_best(tm, gs, best);
 
@@ -896,7 +896,8 @@ __device__ void finalize_period(const SearchArgs& a, GroupSmem& gs, const Team& 
                 o_t0 = fma((double)s / (double)NB, 1.0 / IP, st.t_start);
             }
             double pw, dep, de;
-            window_stats(dw, dy, wtot, ytot, st.s_w, st.s_y, a.objective, &pw, &dep, &de);
+            window_stats(dw, dy, wtot, ytot, st.s_w - st.ew, st.s_y - st.ey, a.objective, &pw, &dep,
+                         &de);
             o_pw = (float)pw;
             o_dep = (float)dep;
             o_de = (float)de;
@@ -925,8 +926,11 @@ __device__ void run_group(const SearchArgs& a, GroupSmem& gs, longlong2* H, cons
         fold_group<GEOM, GLOB, false>(a, gs, HU, so, n_pad, st);
     __syncthreads();
     const int G = gs.G;
+    // teams of tw warps; multi-warp teams synchronise on named barriers 1..15,
+    // so at most 15 of them may exist
     int tw = 1;
     while (tw * 2 * G <= kWarps) tw *= 2;
+    while (tw > 1 && kWarps / tw > 15) tw *= 2;
     const int n_teams = kWarps / tw;
     const int warp = threadIdx.x >> 5;
     Team tm;
@@ -940,7 +944,7 @@ __device__ void run_group(const SearchArgs& a, GroupSmem& gs, longlong2* H, cons
 }
 
 template <int GEOM>
-__global__ void __launch_bounds__(kBlock, 1) search_kernel(const SearchArgs a) {
+__global__ void __launch_bounds__(kBlock, kMinBlocks) search_kernel(const SearchArgs a) {
     extern __shared__ __align__(16) longlong2 s_hist[];
     __shared__ GroupSmem gs;
 
@@ -1161,6 +1165,7 @@ struct atb_handle {
     int device = 0;
     int n_sm = 0;
     int smem_optin = 0;
+    int smem_per_sm = 0;
     std::string err;
 };
 
@@ -1255,6 +1260,7 @@ int atb_create(int device, atb_handle** out) {
     cudaSetDevice(device);
     cudaDeviceGetAttribute(&h->n_sm, cudaDevAttrMultiProcessorCount, device);
     cudaDeviceGetAttribute(&h->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    cudaDeviceGetAttribute(&h->smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device);
     *out = h;
     return ATB_OK;
 }
@@ -1385,7 +1391,8 @@ int atb_plan_create(atb_handle* h, const atb_params* prm, const atb_batch* b,
 
     // shared-memory histogram capacity and the global fallback size
     const int static_smem = (int)sizeof(GroupSmem) + 64;
-    int dyn = h->smem_optin - static_smem - 1024;
+    // kMinBlocks CTAs share the SM's shared memory (1 KiB per CTA is reserved)
+    int dyn = std::min(h->smem_optin, h->smem_per_sm / kMinBlocks - 1024) - static_smem;
     dyn = dyn / 16 * 16;
     const int cap = dyn / 16;
     int nb_max = prm->n_bins;

@@ -484,37 +484,45 @@ static inline void eng_consider(eng_cand* best, float num, float den, int32_t ke
     }
 }
 
-/* per-curve float constants of the window search */
+/* Window-search constants.  Prefix sums are exact FP64 values scaled by
+ * 2^-ew (weights) and 2^-ey (flux) with W_total < 2^ew, sum|q_y| <= 2^ey. */
 typedef struct {
-    float inv_w;   /* 1 / W_total (quantised units) */
-    float k_s;     /* 1 / sum|q_y| */
-    float s_tot;   /* S_total * k_s */
-    double thr;    /* 1e-15 in quantised weight units */
+    double wtot, ytot; /* scaled exact totals */
+    float c1;          /* ytot / wtot */
+    double thr;        /* 1e-15 in scaled weight units */
 } eng_consts;
 
-/* FP32 numerator/denominator of one window; returns 0 if the window is skipped */
-static inline int eng_window_score(double dw, double dy, double w_tot, const eng_consts* kc,
-                                   int dip_only, float* num, float* den)
+static int exp_above(double v)
 {
-    const double wo = w_tot - dw;
-    const float u = (float)dw * kc->inv_w;
-    const float v = (float)wo * kc->inv_w;
-    const float a = (float)dy * kc->k_s;
-    const float sig = fmaf(kc->s_tot, u, -a);
+    int e = 0;
+    if (v > 0.0) frexp(v, &e);
+    return e;
+}
+
+/* FP32 num/den of a window (score proportional to the objective):
+ * sigma = (S/W) W_in - S_in, num = sigma^2, den = W_in W_out.  Returns 0 if
+ * the window is skipped. */
+static inline int eng_window_score(double dw, double dy, const eng_consts* kc, int dip_only,
+                                   float* num, float* den)
+{
+    const double wo = kc->wtot - dw;
+    const float fdw = (float)dw;
+    const float fwo = (float)wo;
+    const float sig = fmaf(kc->c1, fdw, -(float)dy);
     if (dip_only && !(sig >= 0.0f)) return 0;
     *num = sig * sig;
-    *den = u * v;
+    *den = fdw * fwo;
     return 1;
 }
 
-/* FP64 statistics of the winning window from exact quantised sums */
-static void eng_finalize(double dw, double dy, double w_tot, double y_tot, int s_w, int s_y,
+/* FP64 statistics of the winning window; dw, dy scaled by 2^-ew, 2^-ey */
+static void eng_finalize(double dw, double dy, double wtot, double ytot, int s_w, int s_y,
                          int objective, double* power, double* depth, double* derr)
 {
     const double w_in = ldexp(dw, -s_w);
-    const double w_out = ldexp(w_tot - dw, -s_w);
+    const double w_out = ldexp(wtot - dw, -s_w);
     const double s_in = ldexp(dy, -s_y);
-    const double s_out = ldexp(y_tot - dy, -s_y);
+    const double s_out = ldexp(ytot - dy, -s_y);
     const double y_in = s_in / w_in;
     const double y_out = s_out / w_out;
     const double dep = y_out - y_in;
@@ -532,15 +540,6 @@ static void eng_finalize(double dw, double dy, double w_tot, double y_tot, int s
     *power = pw > 0.0 ? pw : 0.0;
     *depth = dep;
     *derr = de;
-}
-
-static void eng_curve_consts(const orc_stage_stats* st, double w_tot, double y_tot, eng_consts* kc)
-{
-    const double ay = st->qy_abs > 0 ? (double)st->qy_abs : 1.0;
-    kc->inv_w = (float)(1.0 / w_tot);
-    kc->k_s = (float)(1.0 / ay);
-    kc->s_tot = (float)(y_tot / ay);
-    kc->thr = ldexp(1e-15, st->s_w);
 }
 
 int orc_eng_binned(int64_t n, const double* dt, const int32_t* qw, const int32_t* qy,
@@ -566,9 +565,13 @@ int orc_eng_binned(int64_t n, const double* dt, const int32_t* qw, const int32_t
         if (periods[p] > pmax) pmax = periods[p];
     int64_t cap = (int64_t)ceil(pmax * inv_bin_dur) + oversample + 2;
     if (max_bins > 0 && cap > max_bins + 2) cap = max_bins + 2;
-    const double w_tot = (double)st->qw_tot, y_tot = (double)st->qy_tot;
+    const int ew = exp_above((double)st->qw_tot), ey = exp_above((double)st->qy_abs);
+    const double w_tot = ldexp((double)st->qw_tot, -ew), y_tot = ldexp((double)st->qy_tot, -ey);
     eng_consts kc;
-    eng_curve_consts(st, w_tot, y_tot, &kc);
+    kc.wtot = w_tot;
+    kc.ytot = y_tot;
+    kc.c1 = w_tot > 0.0 ? (float)(y_tot / w_tot) : 0.0f;
+    kc.thr = ldexp(1e-15, st->s_w - ew);
 
     int err = ORC_OK;
     set_threads(nthreads);
@@ -604,8 +607,8 @@ int orc_eng_binned(int64_t n, const double* dt, const int32_t* qw, const int32_t
                 for (int j = 0; j <= n_bins; ++j) {
                     aw += hw[j];
                     ay += hy[j];
-                    cw[j] = (double)aw;
-                    cy[j] = (double)ay;
+                    cw[j] = ldexp((double)aw, -ew);
+                    cy[j] = ldexp((double)ay, -ey);
                 }
                 eng_cand best = {-1.0f, 1.0f, INT32_MAX};
                 for (int s = 0; s < n_bins; ++s) {
@@ -616,7 +619,7 @@ int orc_eng_binned(int64_t n, const double* dt, const int32_t* qw, const int32_t
                         const double dy = cy[s + d] - cy[s];
                         if (dw < kc.thr || (w_tot - dw) < kc.thr) continue;
                         float num, den;
-                        if (!eng_window_score(dw, dy, w_tot, &kc, 1, &num, &den)) continue;
+                        if (!eng_window_score(dw, dy, &kc, 1, &num, &den)) continue;
                         eng_consider(&best, num, den, s * nd + k);
                     }
                 }
@@ -628,7 +631,8 @@ int orc_eng_binned(int64_t n, const double* dt, const int32_t* qw, const int32_t
                     const double dw = cw[s + d] - cw[s];
                     const double dy = cy[s + d] - cy[s];
                     double pw, dep, de;
-                    eng_finalize(dw, dy, w_tot, y_tot, st->s_w, st->s_y, objective, &pw, &dep, &de);
+                    eng_finalize(dw, dy, w_tot, y_tot, st->s_w - ew, st->s_y - ey, objective, &pw,
+                                 &dep, &de);
                     const double durv = (double)d * bin_dur;
                     power[p] = (float)pw;
                     depth[p] = (float)dep;
@@ -654,6 +658,7 @@ int orc_eng_fixed(int64_t n, const double* dt, const int32_t* qw, const int32_t*
     if (n <= 0 || np <= 0 || nd <= 0 || n_bins < 2) return ORC_EINVAL;
     int err = ORC_OK;
     const double nbd = (double)n_bins;
+    const int ew = exp_above((double)st->qw_tot), ey = exp_above((double)st->qy_abs);
     set_threads(nthreads);
 #pragma omp parallel
     {
@@ -682,14 +687,17 @@ int orc_eng_fixed(int64_t n, const double* dt, const int32_t* qw, const int32_t*
                 for (int j = 0; j <= n_bins; ++j) {
                     aw += hw[j];
                     ay += hy[j];
-                    cw[j] = (double)aw;
-                    cy[j] = (double)ay;
+                    cw[j] = ldexp((double)aw, -ew);
+                    cy[j] = ldexp((double)ay, -ey);
                 }
                 const double w_tot = cw[n_bins], y_tot = cy[n_bins];
                 eng_cand best = {-1.0f, 1.0f, INT32_MAX};
                 if (w_tot > 0.0) {
                     eng_consts kc;
-                    eng_curve_consts(st, w_tot, y_tot, &kc);
+                    kc.wtot = w_tot;
+                    kc.ytot = y_tot;
+                    kc.c1 = (float)(y_tot / w_tot);
+                    kc.thr = 0.0;
                     for (int s = 0; s < n_bins; ++s) {
                         for (int k = 0; k < nd; ++k) {
                             int L = (int)fma(durations[k] * inv_p, nbd, 0.5);
@@ -705,7 +713,7 @@ int orc_eng_fixed(int64_t n, const double* dt, const int32_t* qw, const int32_t*
                             }
                             if (!(dw > 0.0 && dw < w_tot)) continue;
                             float num, den;
-                            eng_window_score(dw, dy, w_tot, &kc, 0, &num, &den);
+                            eng_window_score(dw, dy, &kc, 0, &num, &den);
                             eng_consider(&best, num, den, s * nd + k);
                         }
                     }
@@ -726,7 +734,8 @@ int orc_eng_fixed(int64_t n, const double* dt, const int32_t* qw, const int32_t*
                         dy = (y_tot - cy[s]) + cy[s + L - n_bins];
                     }
                     double pw, dep, de;
-                    eng_finalize(dw, dy, w_tot, y_tot, st->s_w, st->s_y, OBJ_FAST, &pw, &dep, &de);
+                    eng_finalize(dw, dy, w_tot, y_tot, st->s_w - ew, st->s_y - ey, OBJ_FAST, &pw,
+                                 &dep, &de);
                     const double p_ = 1.0 / inv_p;
                     power[p] = (float)pw;
                     depth[p] = (float)dep;
