@@ -29,6 +29,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -1781,3 +1782,267 @@ int atb_bench_dfma(atb_handle* h, double* fma_per_s) {
 }
 
 }  // extern "C"
+
+// ============================================================================
+// Single-curve search that allocates nothing
+// ============================================================================
+//
+// Every buffer the search needs beyond the caller's inputs and outputs lives in
+// one file-scope device array: the staged points of the curve, its constants,
+// the one-curve index arrays, the work-queue counter and the status word.  The
+// array exists once per device that loads this library and stays resident
+// until the process exits.
+
+namespace {
+
+constexpr long long kStaticPoints = ATB_STATIC_MAX_POINTS;
+constexpr size_t kStaticMetaBytes = 4096;
+constexpr size_t kStaticBytes = (size_t)kStaticPoints * 16 + kStaticMetaBytes;
+static_assert(kStaticPoints % kStageAlign == 0, "whole staging chunks");
+
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticBytes];
+
+// byte offsets inside g_static_scratch
+constexpr size_t kOffDt = 0;
+constexpr size_t kOffQw = (size_t)kStaticPoints * 8;
+constexpr size_t kOffQy = (size_t)kStaticPoints * 12;
+constexpr size_t kOffMeta = (size_t)kStaticPoints * 16;
+
+struct StaticMeta {
+    long long pt_off[2];
+    long long t_off[1];
+    long long stage_off[1];
+    long long per_beg[1];
+    long long per_cnt[1];
+    long long dur_beg[1];
+    long long out_beg[1];
+    long long tile_off[2];
+    unsigned long long tile_counter;
+    int dur_cnt[1];
+    int order[1];
+    int status;
+    int nb_max;
+    int dbins[kMaxDur];
+    CurveStat stats[1];
+};
+static_assert(sizeof(StaticMeta) <= kStaticMetaBytes, "static metadata fits its slot");
+
+constexpr int kMaxStaticDevices = 64;
+std::atomic<unsigned char*> g_static_ptr[kMaxStaticDevices];
+
+// one-curve index arrays and the counters that must start at zero
+__global__ void static_meta_init(StaticMeta* m, long long n, long long n_periods, int nd,
+                                 long long n_tiles) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    m->pt_off[0] = 0;
+    m->pt_off[1] = n;
+    m->t_off[0] = 0;
+    m->stage_off[0] = 0;
+    m->per_beg[0] = 0;
+    m->per_cnt[0] = n_periods;
+    m->dur_beg[0] = 0;
+    m->out_beg[0] = 0;
+    m->tile_off[0] = 0;
+    m->tile_off[1] = n_tiles;
+    m->tile_counter = 0ULL;
+    m->dur_cnt[0] = nd;
+    m->order[0] = 0;
+    m->status = 0;
+    m->nb_max = 0;
+}
+
+int static_fail(char* err, size_t err_len, int code, const char* fmt, ...) {
+    if (err && err_len) {
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(err, err_len, fmt, ap);
+        va_end(ap);
+    }
+    return code;
+}
+
+}  // namespace
+
+extern "C" int atb_search_curve_static(const atb_params* prm, const double* t, const void* y,
+                                       int32_t y_is_f64, const float* w, int64_t n,
+                                       const double* periods, int64_t n_periods,
+                                       const double* durations, int32_t n_durations,
+                                       float* power, float* depth, float* depth_err, double* t0,
+                                       float* duration, int32_t* window, int32_t* best_index,
+                                       void* stream, char* err, size_t err_len) {
+    if (err && err_len) err[0] = '\0';
+    if (!prm || !t || !y || !periods || !durations || !power)
+        return static_fail(err, err_len, ATB_EINVAL, "null argument");
+    if (n < 1 || n > kStaticPoints)
+        return static_fail(err, err_len, ATB_EINVAL,
+                           "n=%lld points outside [1, %lld] (the static scratch limit)",
+                           (long long)n, (long long)kStaticPoints);
+    if (n_periods < 1 || n_periods > (1LL << 30))
+        return static_fail(err, err_len, ATB_EINVAL, "n_periods=%lld out of range",
+                           (long long)n_periods);
+    if (n_durations < 1 || n_durations > kMaxDur)
+        return static_fail(err, err_len, ATB_EINVAL, "n_durations=%d outside [1, %d]",
+                           n_durations, kMaxDur);
+    if (prm->geometry == ATB_GEOM_FIXED) {
+        if (prm->objective != ATB_OBJ_FAST)
+            return static_fail(err, err_len, ATB_EINVAL, "the fixed-bin geometry uses the fast objective");
+        if (prm->n_bins < 2 || prm->n_bins > (1 << 24))
+            return static_fail(err, err_len, ATB_EINVAL, "n_bins=%d out of range", prm->n_bins);
+    } else if (prm->geometry == ATB_GEOM_BINNED) {
+        if (prm->objective != ATB_OBJ_SNR && prm->objective != ATB_OBJ_LIKELIHOOD)
+            return static_fail(err, err_len, ATB_EINVAL,
+                               "the binned geometry uses the snr or likelihood objective");
+        if (prm->oversample < 1 || prm->oversample > 1000)
+            return static_fail(err, err_len, ATB_EINVAL, "oversample=%d out of range", prm->oversample);
+        if (prm->max_bins != 0 && prm->max_bins < prm->oversample + 2)
+            return static_fail(err, err_len, ATB_EINVAL, "max_bins=%d must be 0 or >= oversample+2",
+                               prm->max_bins);
+    } else {
+        return static_fail(err, err_len, ATB_EINVAL, "unknown geometry %d", prm->geometry);
+    }
+
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess)
+        return static_fail(err, err_len, ATB_ECUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
+    if (dev < 0 || dev >= kMaxStaticDevices)
+        return static_fail(err, err_len, ATB_EINVAL, "device %d beyond the supported %d", dev,
+                           kMaxStaticDevices);
+    int n_sm = 0, smem_optin = 0, smem_per_sm = 0;
+    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaDeviceGetAttribute(&smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    const int static_smem = (int)sizeof(GroupSmem) + 64;
+    int dyn = std::min(smem_optin, smem_per_sm / kMinBlocks - 1024) - static_smem;
+    dyn = dyn / 16 * 16;
+    const int cap = dyn / 16;
+
+    // set-up, once per device: the scratch array's device address and the
+    // search kernels' shared-memory limit
+    unsigned char* base = g_static_ptr[dev].load(std::memory_order_acquire);
+    if (!base) {
+        void* ptr = nullptr;
+        e = cudaGetSymbolAddress(&ptr, g_static_scratch);
+        if (e != cudaSuccess || !ptr)
+            return static_fail(err, err_len, ATB_ECUDA, "cudaGetSymbolAddress: %s",
+                               cudaGetErrorString(e));
+        e = cudaFuncSetAttribute(search_kernel<ATB_GEOM_BINNED>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(search_kernel<ATB_GEOM_FIXED>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+        if (e != cudaSuccess)
+            return static_fail(err, err_len, ATB_ECUDA, "cudaFuncSetAttribute: %s",
+                               cudaGetErrorString(e));
+        base = static_cast<unsigned char*>(ptr);
+        g_static_ptr[dev].store(base, std::memory_order_release);
+    }
+    double* sdt = reinterpret_cast<double*>(base + kOffDt);
+    int* sqw = reinterpret_cast<int*>(base + kOffQw);
+    int* sqy = reinterpret_cast<int*>(base + kOffQy);
+    StaticMeta* m = reinterpret_cast<StaticMeta*>(base + kOffMeta);
+
+    const long long n_tiles = (n_periods + kTileP - 1) / kTileP;
+    static_meta_init<<<1, 32, 0, s>>>(m, n, n_periods, n_durations, n_tiles);
+
+    int nb_max = prm->n_bins;
+    if (prm->geometry == ATB_GEOM_BINNED) {
+        nbins_max_kernel<<<1, 256, 0, s>>>(1, m->per_beg, m->per_cnt, m->dur_beg, m->dur_cnt,
+                                           periods, durations, prm->oversample, prm->max_bins,
+                                           &m->nb_max);
+        e = cudaMemcpyAsync(&nb_max, &m->nb_max, sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess)
+            return static_fail(err, err_len, ATB_ECUDA, "bin count: %s", cudaGetErrorString(e));
+    }
+    if (nb_max + 2 > cap)
+        return static_fail(err, err_len, ATB_EINVAL,
+                           "a period needs %d bins; this entry point holds at most %d per period "
+                           "(use the plan API)", nb_max, cap - 2);
+    if ((long long)nb_max * n_durations >= (1LL << 31))
+        return static_fail(err, err_len, ATB_EINVAL, "bins x durations too large");
+
+    StageArgs sa{};
+    sa.pt_off = m->pt_off;
+    sa.t_off = m->t_off;
+    sa.stage_off = m->stage_off;
+    sa.dur_beg = m->dur_beg;
+    sa.dur_cnt = m->dur_cnt;
+    sa.t = t;
+    sa.y = y;
+    sa.w = w;
+    sa.durations = durations;
+    sa.sdt = sdt;
+    sa.sqw = sqw;
+    sa.sqy = sqy;
+    sa.stats = m->stats;
+    sa.dbins = m->dbins;
+    sa.oversample = prm->geometry == ATB_GEOM_BINNED ? prm->oversample : 1;
+    sa.status = &m->status;
+    if (y_is_f64)
+        stage_kernel<double><<<1, kStageBlock, 0, s>>>(sa);
+    else
+        stage_kernel<float><<<1, kStageBlock, 0, s>>>(sa);
+
+    SearchArgs qa{};
+    qa.objective = prm->objective;
+    qa.n_bins_fixed = prm->n_bins;
+    qa.oversample = sa.oversample;
+    qa.max_bins = prm->max_bins;
+    qa.n_curves = 1;
+    qa.cap = cap;
+    qa.n_tiles = n_tiles;
+    qa.pt_off = m->pt_off;
+    qa.stage_off = m->stage_off;
+    qa.per_beg = m->per_beg;
+    qa.per_cnt = m->per_cnt;
+    qa.dur_beg = m->dur_beg;
+    qa.dur_cnt = m->dur_cnt;
+    qa.out_beg = m->out_beg;
+    qa.tile_off = m->tile_off;
+    qa.order = m->order;
+    qa.periods = periods;
+    qa.durations = durations;
+    qa.sdt = sdt;
+    qa.sqw = sqw;
+    qa.sqy = sqy;
+    qa.stats = m->stats;
+    qa.dbins = m->dbins;
+    qa.power = power;
+    qa.depth = depth;
+    qa.depth_err = depth_err;
+    qa.t0 = t0;
+    qa.duration = duration;
+    qa.window = window;
+    qa.ghist = nullptr;  // never reached: every period fits shared memory (checked above)
+    qa.ghist_stride = 0;
+    qa.tile_counter = &m->tile_counter;
+    qa.status = &m->status;
+    int occ = 1;
+    if (prm->geometry == ATB_GEOM_BINNED)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, search_kernel<ATB_GEOM_BINNED>, kBlock, dyn);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, search_kernel<ATB_GEOM_FIXED>, kBlock, dyn);
+    const int grid = (int)std::max(1LL, std::min((long long)n_sm * std::max(occ, 1), n_tiles));
+    if (prm->geometry == ATB_GEOM_BINNED)
+        search_kernel<ATB_GEOM_BINNED><<<grid, kBlock, dyn, s>>>(qa);
+    else
+        search_kernel<ATB_GEOM_FIXED><<<grid, kBlock, dyn, s>>>(qa);
+    if (best_index) best_kernel<<<1, 32, 0, s>>>(1, m->per_cnt, m->out_beg, power, best_index);
+    e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return static_fail(err, err_len, ATB_ECUDA, "launch: %s", cudaGetErrorString(e));
+    int status = 0;
+    e = cudaMemcpyAsync(&status, &m->status, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess)
+        return static_fail(err, err_len, ATB_ECUDA, "search: %s", cudaGetErrorString(e));
+    if (status & 1)
+        return static_fail(err, err_len, ATB_EDATA, "input contains non-finite values or weights <= 0");
+    if (status & 2)
+        return static_fail(err, err_len, ATB_EDATA, "durations must be positive and finite");
+    if (status & 4)
+        return static_fail(err, err_len, ATB_EDATA, "periods must be positive and finite");
+    return ATB_OK;
+}

@@ -189,6 +189,40 @@ int atb_debug_fold(atb_handle* h, const atb_params* params, const double* t, con
                    const double* durations, int32_t n_durations, int32_t* out_slots,
                    void* stream);
 
+/*
+ * Single-curve search that allocates nothing.  No counterpart in the
+ * reference: it exists for callers that cannot allocate device memory while
+ * they run -- a host application that has already reserved (nearly) all of the
+ * GPU's memory for its own pool, or a latency-critical loop where cudaMalloc
+ * and cudaFree (which may synchronise the whole device) are not allowed.
+ *
+ * The caller passes device inputs and outputs as for atb_run_gpu_bls /
+ * atb_run_vbls_exact_parity (y is float32, or float64 when y_is_f64; w may be
+ * NULL; any output except power may be NULL; best_index is a DEVICE int32 or
+ * NULL).  All other working memory is one array built into the library,
+ * ATB_STATIC_SCRATCH_BYTES large, that every GPU which loads the library holds
+ * until the process exits.  Limits: at most ATB_STATIC_MAX_POINTS points, at
+ * most 32 durations, and every period's bin count must fit the search kernel's
+ * shared-memory histograms (larger ones are rejected; use the plan API).
+ * Errors are written to err (err_len bytes, may be NULL); no exception, no
+ * allocation on host or device.
+ *
+ * The call is synchronous on `stream`.  The first call on a device looks up
+ * the array's device address and sets the kernels' shared-memory limit; make
+ * that first call before any stream capture.  Every call uses the same array
+ * (the previous call's contents remain; the call resets what must start at
+ * zero), so calls on the same device must not overlap on the GPU: concurrent
+ * calls from several streams or threads race and corrupt each other's results.
+ */
+#define ATB_STATIC_MAX_POINTS 65536
+#define ATB_STATIC_SCRATCH_BYTES (16 * ATB_STATIC_MAX_POINTS + 4096)
+int atb_search_curve_static(const atb_params* params, const double* t, const void* y,
+                            int32_t y_is_f64, const float* w, int64_t n, const double* periods,
+                            int64_t n_periods, const double* durations, int32_t n_durations,
+                            float* power, float* depth, float* depth_err, double* t0,
+                            float* duration, int32_t* window, int32_t* best_index, void* stream,
+                            char* err, size_t err_len);
+
 #ifdef __cplusplus
 }
 #endif
