@@ -127,6 +127,18 @@ class ClockSampler:
                 "samples": len(self.rows)}
 
 
+def measured_traffic(n_curves):
+    """DRAM bytes per search launch from the committed ncu capture, scaled to
+    this launch's number of curves (traffic grows in proportion), or None."""
+    path = os.path.join(ROOT, "profiles", "search_kernel_uniform_batch.json")
+    try:
+        with open(path) as f:
+            prof = json.load(f)
+        return prof["dram_bytes_per_launch"] * n_curves / prof["capture_curves"]
+    except (OSError, KeyError, ValueError):
+        return None
+
+
 def make_workload(args, rank):
     import recipes as R
     t, y, dy, truth = R.uniform_batch(n_curves=args.curves, n=args.points, seed=1000 + rank)
@@ -281,7 +293,7 @@ def main():
         "roofline": {
             "bound": "smem", "kernel": "search_kernel<BINNED>",
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": None,
+            "traffic": measured_traffic(nc),
             "units": f"{ALG_BYTES_PER_FOLD} B of 64-bit shared-memory accumulation per "
                      f"(point, period) fold update; {u_fold:.3e} updates per launch",
             "peak_source": "atb_bench_smem_red_u64 (conflict-free 64-bit shared-memory "
