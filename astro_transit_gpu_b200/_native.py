@@ -33,6 +33,7 @@ EXPORTS = (
     "atb_plan_scratch_bytes", "atb_plan_destroy", "atb_search", "atb_run_gpu_bls",
     "atb_run_vbls_exact_parity", "atb_debug_fold", "atb_plan_profile",
     "atb_bench_smem_red_u64", "atb_bench_dfma", "atb_search_curve_static",
+    "atb_plan_curve_layout",
 )
 
 # limit of atb_search_curve_static (ATB_STATIC_MAX_POINTS in the header)
@@ -99,6 +100,7 @@ def load(build_if_missing: bool = True):
         L.atb_plan_kernel_count.argtypes = [_vp]
         L.atb_plan_scratch_bytes.argtypes = [_vp]
         L.atb_plan_scratch_bytes.restype = _i64
+        L.atb_plan_curve_layout.argtypes = [_vp, _i32p, _i32p]
         L.atb_plan_destroy.argtypes = [_vp]
         L.atb_plan_destroy.restype = None
         L.atb_search.argtypes = [_vp, ctypes.POINTER(Params), ctypes.POINTER(Batch),

@@ -67,6 +67,24 @@ constexpr int kStageBlock = 256;
 constexpr double kMagicRound = 4503599627370496.0;  // 2^52: x + 2^52 (rz) truncates x in [0, 2^31)
 constexpr double kMagicFloor = 6755399441055744.0;  // 1.5*2^52: (m + C)(rd) - C = floor(m), |m| < 2^50
 
+// Histogram word layouts (per curve):
+//   kPackSplit  weights not uniform: words (x, y) = weight sums split at
+//               `lobits`, (z, w) = flux sums split the same way
+//   kPackCount  uniform weights: x = point count, (z, w) = flux sums split
+//   kPackTight  uniform weights and at most M < 2^12 points can share a bin
+//               (b = bits of M): x = count * 2^(32-b) + sum(q mod 2^(32-2b)),
+//               z = sum(q >> (32-2b)); neither word can overflow, and a point
+//               costs two shared-memory reductions instead of three.
+//               M = (floor(T / P_min) + 3) * K, with T the curve's time span and
+//               K the most points inside any time window one bin wide: points
+//               of one bin in one cycle lie in such a window, and the rounded
+//               cycle index takes at most floor(T / P) + 2 values.  High words
+//               sum to < M * 2^(26 - lobits) <= 2^(3b - 6) <= 2^30.
+constexpr int kPackSplit = 0;
+constexpr int kPackCount = 1;
+constexpr int kPackTight = 2;
+constexpr int kTightMaxBits = 12;
+
 // Per-curve fixed-point layout.  Point values are quantised to |q| <= 2^qbits;
 // histogram words hold the low `lobits` bits and the arithmetic-shifted high
 // part of each value in separate 32-bit counters, sized so neither can
@@ -94,7 +112,9 @@ struct CurveStat {
                     // quantised weight unit: "W < 1e-15" is then "W == 0"
     int ew;         // prefix sums are stored as exact FP64 values scaled by 2^-ew (weights)
     int ey;         // and 2^-ey (flux), so that |W| < 1 and |S| <= 1
-    int pad2;
+    int packmode;   // histogram word layout, see kPack*
+    int cshift;     // kPackTight: bit position of the point count in word x
+    int occ_bits;   // bits of the bin-occupancy bound M (64: none)
 };
 
 struct StageArgs {
@@ -114,6 +134,13 @@ struct StageArgs {
     int* dbins;  // [n_curves * kMaxDur]
     int oversample;
     int* status;
+    // period grids, for the bin-occupancy bound of kPackTight (NULL: no bound)
+    const double* periods;
+    const long long* per_beg;
+    const long long* per_cnt;
+    int geometry;
+    int n_bins_fixed;
+    int max_bins;
 };
 
 struct SearchArgs {
@@ -264,6 +291,68 @@ __device__ long long block_sum_ll(long long v, long long* sh) {
 // stage kernel: one CTA per light curve
 // ----------------------------------------------------------------------------
 
+// Bits of a bound M on the number of points of curve c that can share one
+// histogram bin in any period of its grid (64 when no bound is available):
+//   M = (floor(T / P_min) + 3) * K,
+// T = time span, K = most points inside any closed time window of one bin width
+// (astropy-binned: min(duration)/oversample; fixed: P_max/n_bins), widened by a
+// relative 1e-6 for rounding.  Requires time-ordered points.
+__device__ int occupancy_bits(const StageArgs& a, int c, const double* t, long long n, double* shd,
+                              long long* shl) {
+    // time order
+    int unsorted = 0;
+    for (long long i = threadIdx.x; i + 1 < n; i += kStageBlock) unsorted |= t[i] > t[i + 1];
+    if (__syncthreads_or(unsorted)) return 64;
+    // grid extremes
+    const double* per = a.periods + a.per_beg[c];
+    const long long np = a.per_cnt[c];
+    double pmax = 0.0, pinv = 0.0;
+    for (long long i = threadIdx.x; i < np; i += kStageBlock) {
+        const double P = per[i];
+        if (P > 0.0 && P < 1.0e300) {
+            pmax = max(pmax, P);
+            pinv = max(pinv, 1.0 / P);
+        }
+    }
+    pmax = block_max_d(pmax, shd);
+    pinv = block_max_d(pinv, shd);
+    if (!(pinv > 0.0)) return 64;
+    double width;
+    if (a.geometry == ATB_GEOM_BINNED) {
+        const double* dur = a.durations + a.dur_beg[c];
+        double min_dur = dur[0];
+        for (int k = 1; k < a.dur_cnt[c]; ++k) min_dur = min(min_dur, dur[k]);
+        width = min_dur / (double)a.oversample;
+    } else {
+        width = pmax / (double)a.n_bins_fixed;
+    }
+    if (!(width > 0.0) || !isfinite(width)) return 64;
+    width = width * (1.0 + 1e-6) + 1e-12;
+    // K: each thread scans a contiguous range of window starts with a second pointer
+    const long long per_thr = (n + kStageBlock - 1) / kStageBlock;
+    const long long i0 = min(n, (long long)threadIdx.x * per_thr);
+    const long long i1 = min(n, i0 + per_thr);
+    long long kmax = 0;
+    if (i0 < i1) {
+        long long lo = i0, hi = n;  // first j with t[j] > t[i0] + width
+        while (lo < hi) {
+            const long long mid = (lo + hi) >> 1;
+            if (t[mid] - t[i0] <= width) lo = mid + 1; else hi = mid;
+        }
+        long long j = lo;
+        for (long long i = i0; i < i1; ++i) {
+            while (j < n && t[j] - t[i] <= width) ++j;
+            kmax = max(kmax, j - i);
+        }
+    }
+    kmax = (long long)block_max_d((double)kmax, shd);
+    const double span = n > 0 ? t[n - 1] - t[0] : 0.0;
+    const double cycles = floor(span * pinv * (1.0 + 1e-9)) + 3.0;
+    const double m = cycles * (double)kmax;
+    if (!(m < 4096.0)) return 64;
+    return bitlen64((long long)m);
+}
+
 template <typename YT>
 __global__ void __launch_bounds__(kStageBlock) stage_kernel(const StageArgs a) {
     __shared__ double shd[kStageBlock / 32];
@@ -298,16 +387,30 @@ __global__ void __launch_bounds__(kStageBlock) stage_kernel(const StageArgs a) {
     const int s_w = q_scale(wmax, qbits);
     const int s_a = q_scale(amax, qbits);
 
-    // pass 2: exact integer sums -> the shift c (weighted mean of y)
+    // pass 2: exact integer sums -> the shift c (weighted mean of y); the
+    // range of the quantised weights decides the histogram layout
     long long sqw = 0, sqa = 0;
+    int qw_min = 0x7fffffff, qw_max = -1;
     for (long long i = threadIdx.x; i < n; i += kStageBlock) {
         const double wi = w ? (double)w[i] : 1.0;
         const double yi = (double)y[i];
-        sqw += __double2ll_rn(ldexp(wi, s_w));
+        const long long qa = __double2ll_rn(ldexp(wi, s_w));
+        sqw += qa;
         sqa += __double2ll_rn(ldexp(wi * yi, s_a));
+        qw_min = min(qw_min, (int)qa);
+        qw_max = max(qw_max, (int)qa);
     }
     sqw = block_sum_ll(sqw, shl);
     sqa = block_sum_ll(sqa, shl);
+    qw_max = (int)block_max_d((double)qw_max, shd);
+    qw_min = -(int)block_max_d(-(double)qw_min, shd);
+    const bool uniform = n > 0 && qw_min == qw_max;
+    int packmode = uniform ? kPackCount : kPackSplit;
+    int tight_bits = 64;
+    if (uniform && a.periods && !(a.geometry == ATB_GEOM_BINNED && a.max_bins > 0))
+        tight_bits = occupancy_bits(a, c, t, n, shd, shl);
+    if (uniform && tight_bits <= kTightMaxBits && qbits <= 26) packmode = kPackTight;
+    const int qbits_y = qbits;
     const double shift = sqw != 0 ? ldexp((double)sqa / (double)sqw, s_w - s_a) : 0.0;
 
     // pass 3: magnitude of w*(y - c)
@@ -317,11 +420,10 @@ __global__ void __launch_bounds__(kStageBlock) stage_kernel(const StageArgs a) {
         vmax = max(vmax, fabs(wi * ((double)y[i] - shift)));
     }
     vmax = block_max_d(vmax, shd);
-    const int s_y = q_scale(vmax, qbits);
+    const int s_y = q_scale(vmax, qbits_y);
 
     // pass 4: staged arrays (padded with zero-weight points) and totals
     long long qw_tot = 0, qy_tot = 0, qy_abs = 0;
-    int qw_min = 0x7fffffff, qw_max = -1;
     for (long long i = threadIdx.x; i < n_pad; i += kStageBlock) {
         double d = 0.0;
         int qa = 0, qb = 0;
@@ -330,8 +432,6 @@ __global__ void __launch_bounds__(kStageBlock) stage_kernel(const StageArgs a) {
             qa = (int)__double2ll_rn(ldexp(wi, s_w));
             qb = (int)__double2ll_rn(ldexp(wi * ((double)y[i] - shift), s_y));
             d = t[i] - t_start;
-            qw_min = min(qw_min, qa);
-            qw_max = max(qw_max, qa);
         }
         a.sdt[so + i] = d;
         a.sqw[so + i] = qa;
@@ -343,8 +443,6 @@ __global__ void __launch_bounds__(kStageBlock) stage_kernel(const StageArgs a) {
     qw_tot = block_sum_ll(qw_tot, shl);
     qy_tot = block_sum_ll(qy_tot, shl);
     qy_abs = block_sum_ll(qy_abs, shl);
-    qw_max = (int)block_max_d((double)qw_max, shd);
-    qw_min = -(int)block_max_d(-(double)qw_min, shd);
 
     if (threadIdx.x == 0) {
         const int nd = a.dur_cnt[c];
@@ -367,9 +465,9 @@ __global__ void __launch_bounds__(kStageBlock) stage_kernel(const StageArgs a) {
         st.inv_bin_dur = ibd;
         st.dt_absmax = tmax;
         st.n_dur = nd;
-        st.qbits = qbits;
+        st.qbits = qbits_y;
         st.lobits = curve_lobits(n);
-        st.uniform_w = (n > 0 && qw_min == qw_max) ? 1 : 0;
+        st.uniform_w = uniform ? 1 : 0;
         st.qw0 = n > 0 ? qw_max : 0;
         st.thr_unit = ldexp(1e-15, s_w) < 1.0 ? 1 : 0;
         int ew = 0, ey = 0;
@@ -377,7 +475,14 @@ __global__ void __launch_bounds__(kStageBlock) stage_kernel(const StageArgs a) {
         if (qy_abs > 0) frexp((double)qy_abs, &ey);
         st.ew = ew;
         st.ey = ey;
-        st.pad2 = 0;
+        st.packmode = packmode;
+        if (packmode == kPackTight) {
+            st.lobits = 32 - 2 * tight_bits;
+            st.cshift = 32 - tight_bits;
+        } else {
+            st.cshift = 0;
+        }
+        st.occ_bits = tight_bits;
         a.stats[c] = st;
     }
 }
@@ -422,25 +527,6 @@ __device__ __forceinline__ void store_components(uint4* H, int s, uint4 e) {
         e.x = e.z; e.y = e.w; e.z = t0; e.w = t1;
     }
     H[s] = e;
-}
-
-template <bool GLOB, bool UNI>
-__device__ __forceinline__ void hist_add(uint4* H, int slot, unsigned dwl, unsigned dwh, unsigned dyl,
-                                         unsigned dyh) {
-    const unsigned r = slot_rot(slot);
-    if (GLOB) {
-        unsigned* e = reinterpret_cast<unsigned*>(H + slot);
-        atomicAdd(e + (0u ^ r), dwl);
-        if (!UNI) atomicAdd(e + (1u ^ r), dwh);
-        atomicAdd(e + (2u ^ r), dyl);
-        atomicAdd(e + (3u ^ r), dyh);
-    } else {
-        const unsigned b = (unsigned)__cvta_generic_to_shared(H + slot) | (r << 2);
-        red_shared_u32(b, dwl);
-        if (!UNI) red_shared_u32(b ^ 4u, dwh);
-        red_shared_u32(b ^ 8u, dyl);
-        red_shared_u32(b ^ 12u, dyh);
-    }
 }
 
 struct Team {
@@ -536,7 +622,32 @@ __device__ __forceinline__ void fold_slots(const double (&d)[kR], bool sorted, b
 }
 
 // fold every staged point of the curve into the group's histograms
-template <int GEOM, bool GLOB, bool UNI>
+// Add one point's words to histogram entry `slot` (component c of the entry
+// lives at word c ^ rot(slot)).  MODE selects the layout (kPack*); words a..d
+// are the point's components x, y, z, w (unused ones are ignored).
+template <bool GLOB, int MODE>
+__device__ __forceinline__ void hist_add_point(uint4* H, int slot, unsigned a, unsigned b,
+                                               unsigned c, unsigned d) {
+    const unsigned r = slot_rot(slot);
+    if (GLOB) {
+        unsigned* e = reinterpret_cast<unsigned*>(H + slot);
+        atomicAdd(e + (0u ^ r), a);
+        if (MODE == kPackSplit) atomicAdd(e + (1u ^ r), b);
+        atomicAdd(e + (2u ^ r), c);
+        if (MODE != kPackTight) atomicAdd(e + (3u ^ r), d);
+    } else {
+        const unsigned ad = (unsigned)__cvta_generic_to_shared(H + slot) | (r << 2);
+        red_shared_u32(ad, a);
+        if (MODE == kPackSplit) red_shared_u32(ad ^ 4u, b);
+        red_shared_u32(ad ^ 8u, c);
+        if (MODE != kPackTight) red_shared_u32(ad ^ 12u, d);
+    }
+}
+
+// Fold every staged point of the curve into the group's histograms: one
+// reduction per histogram word and point (merging runs of equal bins costs
+// more issue slots than the reductions it saves).
+template <int GEOM, bool GLOB, int MODE>
 __device__ void fold_group(const SearchArgs& a, const GroupSmem& gs, uint4* H, long long so,
                            long long n_pad, const CurveStat& st) {
     const int G = gs.G;
@@ -567,21 +678,20 @@ __device__ void fold_group(const SearchArgs& a, const GroupSmem& gs, uint4* H, l
         bool sorted = true;
 #pragma unroll
         for (int j = 0; j + 1 < kR; ++j) sorted = sorted && (d[j] <= d[j + 1]);
-        // running sums of the split words over the thread's points
-        unsigned pwl[kR], pwh[kR], pyl[kR], pyh[kR];
-        {
-            unsigned aw = 0, bw = 0, ay = 0, by = 0;
+        // each point's histogram words (padding points have q_w = q_y = 0)
+        unsigned wa[kR], wb[kR], wc[kR], wd[kR];
 #pragma unroll
-            for (int j = 0; j < kR; ++j) {
-                if (UNI) {
-                    aw += qw[j] != 0 ? 1u : 0u;  // padding points carry q_w = 0
-                } else {
-                    aw += (unsigned)qw[j] & lomask;
-                    bw += (unsigned)(qw[j] >> L);
-                }
-                ay += (unsigned)qy[j] & lomask;
-                by += (unsigned)(qy[j] >> L);
-                pwl[j] = aw; pwh[j] = bw; pyl[j] = ay; pyh[j] = by;
+        for (int j = 0; j < kR; ++j) {
+            if (MODE == kPackTight) {
+                wa[j] = (qw[j] != 0 ? (1u << st.cshift) : 0u) + ((unsigned)qy[j] & lomask);
+                wb[j] = 0u;
+                wc[j] = (unsigned)(qy[j] >> L);
+                wd[j] = 0u;
+            } else {
+                wa[j] = MODE == kPackCount ? (qw[j] != 0 ? 1u : 0u) : ((unsigned)qw[j] & lomask);
+                wb[j] = MODE == kPackCount ? 0u : (unsigned)(qw[j] >> L);
+                wc[j] = (unsigned)qy[j] & lomask;
+                wd[j] = (unsigned)(qy[j] >> L);
             }
         }
         for (int g = 0; g < G; ++g) {
@@ -589,15 +699,8 @@ __device__ void fold_group(const SearchArgs& a, const GroupSmem& gs, uint4* H, l
             int sl[kR];
             fold_slots<GEOM>(d, sorted, safe, gs.P[g], gs.IP[g], st.inv_bin_dur, NB, sl);
             uint4* Hg = H + gs.base[g];
-            unsigned lw = 0, lh = 0, ly = 0, lz = 0;
-            // runs of equal slots are merged: one reduction per run, at its end
 #pragma unroll
-            for (int j = 0; j < kR; ++j) {
-                if (j == kR - 1 || sl[j] != sl[j + 1]) {
-                    hist_add<GLOB, UNI>(Hg, sl[j], pwl[j] - lw, pwh[j] - lh, pyl[j] - ly, pyh[j] - lz);
-                    lw = pwl[j]; lh = pwh[j]; ly = pyl[j]; lz = pyh[j];
-                }
-            }
+            for (int j = 0; j < kR; ++j) hist_add_point<GLOB, MODE>(Hg, sl[j], wa[j], wb[j], wc[j], wd[j]);
         }
     }
 }
@@ -633,10 +736,18 @@ __device__ void window_stats(double dw, double dy, double wtot, double ytot, int
 // (|sum| < 2^53, so both the conversion and the scaling are exact).
 // Threads own contiguous segments of odd length, so the 16-byte entries a
 // warp touches in one step fall in distinct bank groups.
-__device__ __forceinline__ void entry_sums(const uint4 e, int L, bool uni, long long qw0,
-                                           long long& w, long long& y) {
-    w = uni ? (long long)e.x * qw0 : (long long)e.y * (1LL << L) + (long long)e.x;
-    y = (long long)(int)e.w * (1LL << L) + (long long)e.z;
+__device__ __forceinline__ void entry_sums(const uint4* R, int i, const CurveStat& st, long long& w,
+                                           long long& y) {
+    const uint4 e = load_components(R, i);
+    if (st.packmode == kPackTight) {
+        const long long cnt = (long long)(e.x >> st.cshift);
+        w = cnt * (long long)st.qw0;
+        y = (long long)(int)e.z * (1LL << st.lobits) + (long long)(e.x & ((1u << st.cshift) - 1u));
+    } else {
+        w = st.packmode == kPackCount ? (long long)e.x * (long long)st.qw0
+                                      : (long long)e.y * (1LL << st.lobits) + (long long)e.x;
+        y = (long long)(int)e.w * (1LL << st.lobits) + (long long)e.z;
+    }
 }
 
 __device__ void team_scan(const Team& tm, GroupSmem& gs, longlong2* E, int M, const CurveStat& st) {
@@ -644,14 +755,11 @@ __device__ void team_scan(const Team& tm, GroupSmem& gs, longlong2* E, int M, co
     seg |= 1;
     const int b = min(M, tm.tid * seg);
     const int e = min(M, b + seg);
-    const int L = st.lobits;
-    const bool uni = st.uniform_w != 0;
-    const long long qw0 = st.qw0;
     const uint4* R = reinterpret_cast<const uint4*>(E);
     long long sw = 0, sy = 0;
     for (int i = b; i < e; ++i) {
         long long w, y;
-        entry_sums(load_components(R, i), L, uni, qw0, w, y);
+        entry_sums(R, i, st, w, y);
         sw += w;
         sy += y;
     }
@@ -683,7 +791,7 @@ __device__ void team_scan(const Team& tm, GroupSmem& gs, longlong2* E, int M, co
     const double sw2 = ldexp(1.0, -st.ew), sy2 = ldexp(1.0, -st.ey);
     for (int i = b; i < e; ++i) {
         long long w, y;
-        entry_sums(load_components(R, i), L, uni, qw0, w, y);
+        entry_sums(R, i, st, w, y);
         xw += w;
         xy += y;
         E[i] = make_longlong2(__double_as_longlong((double)xw * sw2),
@@ -921,10 +1029,12 @@ __device__ void run_group(const SearchArgs& a, GroupSmem& gs, longlong2* H, cons
     for (int i = threadIdx.x; i < total; i += kBlock) H[i] = make_longlong2(0, 0);
     __syncthreads();
     uint4* HU = reinterpret_cast<uint4*>(H);
-    if (st.uniform_w)
-        fold_group<GEOM, GLOB, true>(a, gs, HU, so, n_pad, st);
+    if (st.packmode == kPackTight)
+        fold_group<GEOM, GLOB, kPackTight>(a, gs, HU, so, n_pad, st);
+    else if (st.packmode == kPackCount)
+        fold_group<GEOM, GLOB, kPackCount>(a, gs, HU, so, n_pad, st);
     else
-        fold_group<GEOM, GLOB, false>(a, gs, HU, so, n_pad, st);
+        fold_group<GEOM, GLOB, kPackSplit>(a, gs, HU, so, n_pad, st);
     __syncthreads();
     const int G = gs.G;
     // teams of tw warps; multi-warp teams synchronise on named barriers 1..15,
@@ -1389,6 +1499,12 @@ int atb_plan_create(atb_handle* h, const atb_params* prm, const atb_batch* b,
     sa.dbins = d_dbins;
     sa.oversample = prm->geometry == ATB_GEOM_BINNED ? prm->oversample : 1;
     sa.status = p->status;
+    sa.periods = b->periods;
+    sa.per_beg = d_pbeg;
+    sa.per_cnt = d_pcnt;
+    sa.geometry = prm->geometry;
+    sa.n_bins_fixed = prm->n_bins;
+    sa.max_bins = prm->max_bins;
 
     // shared-memory histogram capacity and the global fallback size
     const int static_smem = (int)sizeof(GroupSmem) + 64;
@@ -1530,6 +1646,19 @@ int atb_plan_kernel_count(const atb_plan* p) {
 }
 
 int64_t atb_plan_scratch_bytes(const atb_plan* p) { return p ? p->scratch_bytes : 0; }
+
+int atb_plan_curve_layout(atb_plan* p, int32_t* layout, int32_t* occupancy_bits) {
+    if (!p || !layout || !occupancy_bits) return ATB_EINVAL;
+    ATB_CUDA(p->h, cudaSetDevice(p->h->device));
+    std::vector<CurveStat> st(p->n_curves);
+    ATB_CUDA(p->h, cudaMemcpy(st.data(), p->sa.stats, sizeof(CurveStat) * st.size(),
+                              cudaMemcpyDeviceToHost));
+    for (int c = 0; c < p->n_curves; ++c) {
+        layout[c] = st[c].packmode;
+        occupancy_bits[c] = st[c].occ_bits;
+    }
+    return ATB_OK;
+}
 
 int atb_plan_check(atb_plan* p) {
     if (!p) return ATB_EINVAL;
@@ -1980,6 +2109,12 @@ extern "C" int atb_search_curve_static(const atb_params* prm, const double* t, c
     sa.dbins = m->dbins;
     sa.oversample = prm->geometry == ATB_GEOM_BINNED ? prm->oversample : 1;
     sa.status = &m->status;
+    sa.periods = periods;
+    sa.per_beg = m->per_beg;
+    sa.per_cnt = m->per_cnt;
+    sa.geometry = prm->geometry;
+    sa.n_bins_fixed = prm->n_bins;
+    sa.max_bins = prm->max_bins;
     if (y_is_f64)
         stage_kernel<double><<<1, kStageBlock, 0, s>>>(sa);
     else

@@ -241,6 +241,20 @@ class SearchPlan:
         N.raise_for(rc, self.engine.handle.ptr, "plan profile")
         return {"stage": ms[0].value, "search": ms[1].value, "best": ms[2].value}
 
+    def curve_layout(self):
+        """After an execution: (layout, occupancy_bits) per curve, numpy int32.
+        layout is ATB_LAYOUT_SPLIT / COUNT / TIGHT (0 / 1 / 2), the histogram
+        word layout the search used; occupancy_bits is the bit length of the
+        curve's bound on points per bin (64: no bound).  Synchronous."""
+        nc = self.batch.n_curves
+        lay = np.zeros(nc, np.int32)
+        bits = np.zeros(nc, np.int32)
+        rc = self._lib.atb_plan_curve_layout(
+            self.ptr, lay.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+            bits.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)))
+        N.raise_for(rc, self.engine.handle.ptr, "curve layout")
+        return lay, bits
+
     def check(self) -> None:
         """Synchronise and raise ValueError if the last execution saw invalid data."""
         rc = self._lib.atb_plan_check(self.ptr)

@@ -129,6 +129,20 @@ int atb_plan_kernel_count(const atb_plan* p);
 int64_t atb_plan_scratch_bytes(const atb_plan* p);
 void atb_plan_destroy(atb_plan* p);
 
+/*
+ * Diagnostics (no reference counterpart): after an atb_plan_execute has
+ * completed, the histogram word layout each curve used and the bit length of
+ * its bin-occupancy bound (64: no bound).  Layouts: ATB_LAYOUT_SPLIT (weights
+ * not uniform), ATB_LAYOUT_COUNT (uniform weights), ATB_LAYOUT_TIGHT (uniform
+ * weights and fewer than 2^12 points can share a bin: two 32-bit reductions
+ * per point instead of three).  The layout never changes the results.
+ * Synchronous; both arrays hold one entry per curve.
+ */
+#define ATB_LAYOUT_SPLIT 0
+#define ATB_LAYOUT_COUNT 1
+#define ATB_LAYOUT_TIGHT 2
+int atb_plan_curve_layout(atb_plan* p, int32_t* layout, int32_t* occupancy_bits);
+
 /* One-shot: create, execute on `stream`, synchronise, check, destroy. */
 int atb_search(atb_handle* h, const atb_params* params, const atb_batch* batch,
                const atb_outputs* outputs, void* stream);

@@ -115,7 +115,7 @@ def ref_binned(t, y, w, periods, durations, oversample=10, max_bins=0, objective
     out["gap"] = np.zeros(len(periods), np.float64)
     rc = lib().orc_ref_binned(len(t), _ptr(t, _dp), _ptr(y, _dp), _ptr(w, _dp), len(periods),
                               _ptr(periods, _dp), len(durations), _ptr(durations, _dp),
-                              int(oversample), int(max_bins), OBJECTIVES[objective], int(nthreads),
+                              int(oversample), int(max_bins or 0), OBJECTIVES[objective], int(nthreads),
                               *(_ptr(out[k], _dp) for k in ("power", "depth", "depth_err", "t0",
                                                              "duration")),
                               _ptr(out["window"], _ip), _ptr(out["gap"], _dp))
@@ -166,7 +166,7 @@ def eng_binned(t, y, w, periods, durations, oversample=10, max_bins=0, objective
     pb = np.zeros(len(periods) * len(dt), np.int32) if point_bins else None
     rc = lib().orc_eng_binned(len(dt), _ptr(dt, _dp), _ptr(qw, _ip), _ptr(qy, _ip),
                               ctypes.byref(st), len(periods), _ptr(periods, _dp), len(durations),
-                              _ptr(durations, _dp), int(oversample), int(max_bins),
+                              _ptr(durations, _dp), int(oversample), int(max_bins or 0),
                               OBJECTIVES[objective], int(nthreads),
                               _ptr(out["power"], _fp), _ptr(out["depth"], _fp),
                               _ptr(out["depth_err"], _fp), _ptr(out["t0"], _dp),

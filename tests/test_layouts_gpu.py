@@ -1,0 +1,147 @@
+"""GPU tests of the histogram word layouts.
+
+Uniform-weight curves whose bin occupancy is provably below 2^12 points use
+the two-word layout (ATB_LAYOUT_TIGHT); the others use the three- or four-word
+layouts.  The layout must never change a result: every case is bit-exact
+against the oracle's mirror of the engine arithmetic, and for every TIGHT curve
+the largest bin occupancy actually reached (counted from the per-point slots
+of the same fold) stays below the curve's bound.
+"""
+import numpy as np
+import pytest
+
+import recipes as R
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+SPLIT, COUNT, TIGHT = 0, 1, 2
+FIELDS = ("power", "depth", "depth_err", "t0", "duration", "window")
+
+
+def _cfg(kind, **kw):
+    from astro_transit_gpu_b200.engine import SearchConfig
+    if kind == "fixed":
+        return SearchConfig("fast", n_bins=kw.get("n_bins") or 200)
+    return SearchConfig("parity", objective="snr", max_bins=kw.get("max_bins"), oversample=10)
+
+
+def run_with_layout(engine, t, y, w, periods, durations, cfg):
+    from astro_transit_gpu_b200.engine import CurveBatch, split_outputs
+    b = CurveBatch.from_arrays([t], [np.asarray(y, np.float32)], periods=periods,
+                               durations=durations, weights=None if w is None else [w])
+    plan = engine.plan(b, cfg)
+    try:
+        plan.execute()
+        plan.check()
+        lay, bits = plan.curve_layout()
+        out = split_outputs(b, plan.outputs)[0]
+    finally:
+        plan.close()
+    return out, int(lay[0]), int(bits[0])
+
+
+def oracle_for(t, y, w, periods, durs, cfg):
+    y = np.asarray(y, np.float32)
+    if cfg.method == "fast":
+        return O.eng_fixed(t, y, w, periods, durs, n_bins=cfg.n_bins)
+    return O.eng_binned(t, y, w, periods, durs, max_bins=cfg.max_bins or 0)
+
+
+def max_occupancy(engine, t, y, w, periods, durs, cfg):
+    import torch
+    dev = engine.device
+    slots = engine.debug_fold(
+        torch.tensor(t, device=dev), torch.tensor(np.asarray(y, np.float32), device=dev),
+        None if w is None else torch.tensor(w, device=dev), torch.tensor(periods, device=dev),
+        torch.tensor(durs, device=dev), cfg).cpu().numpy()
+    worst = 0
+    for row in slots:
+        cnt = np.bincount(row)
+        if cfg.method == "fast":
+            cnt = cnt[:-1] if cnt.size > 1 else cnt  # the out-of-range slot is never read
+        worst = max(worst, int(cnt.max()))
+    return worst
+
+
+def expected_bits(t, periods, durs, cfg):
+    """The kernel's occupancy bound restated: M = (floor(T/P_min) + 3) * K,
+    K = most points within one (slightly widened) bin width; 64 = no bound."""
+    t = np.asarray(t, np.float64)
+    if np.any(np.diff(t) < 0):
+        return 64
+    if cfg.method == "fast":
+        width = periods.max() / cfg.n_bins
+    elif cfg.max_bins:
+        return 64
+    else:
+        width = durs.min() / cfg.oversample
+    width = width * (1 + 1e-6) + 1e-12
+    k = int((np.searchsorted(t, t + width, side="right") - np.arange(t.size)).max())
+    m = (np.floor((t[-1] - t[0]) * (1 / periods).max() * (1 + 1e-9)) + 3) * k
+    return 64 if m >= 4096 else int(m).bit_length()
+
+
+def clustered(n_clusters=40, per_cluster=60, span=27.0, seed=3):
+    """Uniform weights, tight bursts of simultaneous samples."""
+    rng = np.random.default_rng(seed)
+    centres = np.sort(rng.uniform(0, span, n_clusters))
+    t = np.sort(np.concatenate([c + rng.uniform(0, 1e-4, per_cluster) for c in centres]))
+    y = R.inject_box(t, 1.0 + rng.normal(0, 1e-3, t.size), 3.3, 0.4, 0.12, 3e-3)
+    return t + 2000.0, y
+
+
+CASES = {
+    # name: (t, y, w, periods, durations, kind, n_bins, expected layout)
+    "c0_uniform": lambda: (*R.c0_curve(n=15000, seed=2)[:2], None, R.c0_periods(600),
+                           R.C0_DURATIONS, "binned", None, TIGHT),
+    # fixed 200 bins: bound 3819 points, 12 bits (the largest tight layout)
+    "c0_uniform_fixed": lambda: (*R.c0_curve(n=15000, seed=2)[:2], None, R.c0_periods(600),
+                                 R.C0_DURATIONS, "fixed", 200, TIGHT),
+    # bursts of 60 simultaneous samples: bound 3300 points, bins reach 60+
+    "clustered": lambda: (*clustered(seed=3), None, np.geomspace(0.5, 13.7, 500),
+                          np.array([0.04, 0.1]), "binned", None, TIGHT),
+    "clustered_fixed": lambda: (*clustered(seed=5), None, np.geomspace(0.5, 13.7, 500),
+                                np.array([0.04, 0.1]), "fixed", 2000, TIGHT),
+}
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_tight_layout_bound_holds_and_results_bit_exact(engine, name):
+    t, y, w, periods, durs, kind, n_bins, expect = CASES[name]()
+    cfg = _cfg(kind, n_bins=n_bins)
+    g, lay, bits = run_with_layout(engine, t, y, w, periods, durs, cfg)
+    assert lay == expect, (lay, bits)
+    assert bits == expected_bits(t, periods, durs, cfg) <= 12
+    assert max_occupancy(engine, t, y, w, periods, durs, cfg) < (1 << bits)
+    o = oracle_for(t, y, w, periods, durs, cfg)
+    for k in FIELDS:
+        assert np.array_equal(np.asarray(g[k]), np.asarray(o[k])), (name, k)
+
+
+def test_layout_falls_back_when_no_bound(engine):
+    rng = np.random.default_rng(8)
+    periods, durs = np.geomspace(0.5, 5.0, 200), np.array([0.05, 0.1])
+    # dense: 20000 samples within 0.05 d -> a bound of ~6000 points per bin
+    t = np.sort(rng.uniform(0, 0.05, 20000)) + 10.0
+    y = 1.0 + rng.normal(0, 1e-3, t.size)
+    cases = [
+        (t, y, None, "binned", None, COUNT),
+        # unsorted times: no bound is computed
+        (rng.permutation(R.c0_curve(n=4000, seed=4)[0]), rng.normal(1, 1e-3, 4000), None,
+         "binned", None, COUNT),
+        # the reference's bin cap folds many points into the last bin
+        (*R.c0_curve(n=4000, seed=4)[:2], None, "binned", 2000, COUNT),
+        # non-uniform weights
+        (*R.c0_curve(n=4000, seed=4)[:2], rng.uniform(1e5, 2e5, 4000).astype(np.float32),
+         "binned", None, SPLIT),
+    ]
+    for t_, y_, w_, kind, mb, expect in cases:
+        cfg = _cfg(kind, max_bins=mb)
+        g, lay, bits = run_with_layout(engine, t_, y_, w_, periods, durs, cfg)
+        assert lay == expect, (expect, lay, bits)
+        if w_ is None:
+            assert bits == expected_bits(t_, periods, durs, cfg) == 64
+        o = oracle_for(t_, y_, w_, periods, durs, cfg)
+        for k in FIELDS:
+            assert np.array_equal(np.asarray(g[k]), np.asarray(o[k])), (expect, k)
