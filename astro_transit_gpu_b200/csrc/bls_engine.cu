@@ -115,6 +115,9 @@ struct CurveStat {
     int packmode;   // histogram word layout, see kPack*
     int cshift;     // kPackTight: bit position of the point count in word x
     int occ_bits;   // bits of the bin-occupancy bound M (64: none)
+    int cnt_win;    // uniform weights and fewer than 2^24 points: the window search
+                    // works on exact FP32 point counts instead of FP64 weight sums
+    int n_cnt;      // number of points (cnt_win)
 };
 
 struct StageArgs {
@@ -483,6 +486,8 @@ __global__ void __launch_bounds__(kStageBlock) stage_kernel(const StageArgs a) {
             st.cshift = 0;
         }
         st.occ_bits = tight_bits;
+        st.cnt_win = (uniform && n < (1LL << 24)) ? 1 : 0;
+        st.n_cnt = st.cnt_win ? (int)n : 0;
         a.stats[c] = st;
     }
 }
@@ -730,24 +735,26 @@ __device__ void window_stats(double dw, double dy, double wtot, double ytot, int
     *derr = de;
 }
 
-// Inclusive scan of the raw histogram entries H[0..M) in place: each entry's
-// split 32-bit words are combined into exact int64 sums (W, Y) and the
-// running sums are written back as exact FP64 values scaled by 2^-ew, 2^-ey
-// (|sum| < 2^53, so both the conversion and the scaling are exact).
+// Inclusive scan of the raw histogram entries H[0..M) in place.  Pass 1
+// decodes each entry's split 32-bit words once into exact int64 sums (W, Y)
+// and writes them back; pass 2 adds the running sums and writes exact values:
+// the flux sum as FP64 scaled by 2^-ey, and the weight sum as FP64 scaled by
+// 2^-ew or, for counting curves (cnt_win), the point count as FP32 in the low
+// word (|sum| < 2^53 and counts < 2^24, so every conversion is exact).
 // Threads own contiguous segments of odd length, so the 16-byte entries a
 // warp touches in one step fall in distinct bank groups.
 __device__ __forceinline__ void entry_sums(const uint4* R, int i, const CurveStat& st, long long& w,
                                            long long& y) {
     const uint4 e = load_components(R, i);
     if (st.packmode == kPackTight) {
-        const long long cnt = (long long)(e.x >> st.cshift);
-        w = cnt * (long long)st.qw0;
+        w = (long long)(e.x >> st.cshift);
         y = (long long)(int)e.z * (1LL << st.lobits) + (long long)(e.x & ((1u << st.cshift) - 1u));
     } else {
-        w = st.packmode == kPackCount ? (long long)e.x * (long long)st.qw0
+        w = st.packmode == kPackCount ? (long long)e.x
                                       : (long long)e.y * (1LL << st.lobits) + (long long)e.x;
         y = (long long)(int)e.w * (1LL << st.lobits) + (long long)e.z;
     }
+    if (st.packmode != kPackSplit && !st.cnt_win) w *= (long long)st.qw0;
 }
 
 __device__ void team_scan(const Team& tm, GroupSmem& gs, longlong2* E, int M, const CurveStat& st) {
@@ -760,6 +767,7 @@ __device__ void team_scan(const Team& tm, GroupSmem& gs, longlong2* E, int M, co
     for (int i = b; i < e; ++i) {
         long long w, y;
         entry_sums(R, i, st, w, y);
+        E[i] = make_longlong2(w, y);
         sw += w;
         sy += y;
     }
@@ -788,14 +796,24 @@ __device__ void team_scan(const Team& tm, GroupSmem& gs, longlong2* E, int M, co
         iy += oy;
     }
     long long xw = iw - sw, xy = iy - sy;
-    const double sw2 = ldexp(1.0, -st.ew), sy2 = ldexp(1.0, -st.ey);
-    for (int i = b; i < e; ++i) {
-        long long w, y;
-        entry_sums(R, i, st, w, y);
-        xw += w;
-        xy += y;
-        E[i] = make_longlong2(__double_as_longlong((double)xw * sw2),
-                              __double_as_longlong((double)xy * sy2));
+    const double sy2 = ldexp(1.0, -st.ey);
+    if (st.cnt_win) {
+        for (int i = b; i < e; ++i) {
+            const longlong2 v = E[i];
+            xw += v.x;
+            xy += v.y;
+            E[i] = make_longlong2((long long)__float_as_uint((float)(int)xw),
+                                  __double_as_longlong((double)xy * sy2));
+        }
+    } else {
+        const double sw2 = ldexp(1.0, -st.ew);
+        for (int i = b; i < e; ++i) {
+            const longlong2 v = E[i];
+            xw += v.x;
+            xy += v.y;
+            E[i] = make_longlong2(__double_as_longlong((double)xw * sw2),
+                                  __double_as_longlong((double)xy * sy2));
+        }
     }
     team_sync(tm);
 }
@@ -828,17 +846,22 @@ __device__ Cand team_best(const Team& tm, GroupSmem& gs, Cand c) {
 
 struct WinConsts {
     double wtot, ytot;  // exact totals, scaled like the prefix sums
-    float c1;           // ytot / wtot
+    float c1;           // ytot / wtot, or ytot / N for counting curves
+    float fN;           // counting curves: N, the number of points in the histogram
     double thr;         // 1e-15 in scaled weight units
+    double qw0s;        // counting curves: the scaled weight of one point
 };
 
-// One (start, duration) window from exact scaled FP64 prefix values: returns
-// false when the window is skipped, else FP32 num/den of a score proportional
-// to the objective within the period:
+// One (start, duration) window: returns false when the window is skipped,
+// else FP32 num/den of a score proportional to the objective within the
+// period:
 //   sigma = (S/W) W_in - S_in,  num = sigma^2,  den = W_in W_out
 //   (num/den = depth^2 W_in W_out / W^2, the SNR^2 up to a per-period factor)
 //   BINNED (vbls_v42_parity.cu:103-116): skip empty in/out windows, dip-only
 //   FIXED  (bls.cu:128): skip unless 0 < W_in < W
+// Weighted curves pass exact scaled FP64 weight sums (dw); counting curves
+// pass the exact FP32 point count of the window (fdw) and use N and S/N in
+// place of W and S/W (the same score up to the constant factor qw0s^2).
 template <int GEOM, bool UNIT>
 __device__ __forceinline__ bool window_eval(double dw, double dy, const WinConsts& kc, float& num,
                                             float& den) {
@@ -850,6 +873,23 @@ __device__ __forceinline__ bool window_eval(double dw, double dy, const WinConst
         ok = fdw > 0.0f && fwo > 0.0f;  // exact: dw, wo are scaled integers and thr < 1 unit
     } else {
         ok = !(dw < kc.thr || wo < kc.thr);
+    }
+    const float sig = __fmaf_rn(kc.c1, fdw, -__double2float_rn(dy));
+    if (GEOM == ATB_GEOM_BINNED) ok = ok && (sig >= 0.0f);
+    num = __fmul_rn(sig, sig);
+    den = __fmul_rn(fdw, fwo);
+    return ok;
+}
+
+template <int GEOM, bool UNIT>
+__device__ __forceinline__ bool window_eval_cnt(float fdw, double dy, const WinConsts& kc,
+                                                float& num, float& den) {
+    const float fwo = __fsub_rn(kc.fN, fdw);  // exact: integers below 2^24
+    bool ok;
+    if (UNIT) {
+        ok = fdw > 0.0f && fwo > 0.0f;
+    } else {
+        ok = !((double)fdw * kc.qw0s < kc.thr || (double)fwo * kc.qw0s < kc.thr);
     }
     const float sig = __fmaf_rn(kc.c1, fdw, -__double2float_rn(dy));
     if (GEOM == ATB_GEOM_BINNED) ok = ok && (sig >= 0.0f);
@@ -878,54 +918,101 @@ struct Best {
     }
 };
 
-// All windows of one period over starts tid, tid+nthreads, ...  Durations are
-// taken four at a time: the four end points are loaded before any is used
-// (instruction-level parallelism with few live registers).
-template <int GEOM, bool UNIT>
-__device__ Cand window_search(const longlong2* E, int NB, int nd, const int* lens_smem, int tid,
-                              int nthreads, const WinConsts& kc) {
-    constexpr int kC = 4;
-    Best best;
-    best.init();
-    for (int k0 = 0; k0 < nd; k0 += kC) {
-        int len[kC];
+__device__ __forceinline__ float cnt_of(long long x) { return __int_as_float((int)x); }
+
+// The windows (s, len[k]) of KC durations at one start s.  CHECK = false is
+// the interior, where every window ends at or before bin NB: no clamping, no
+// wrap and no range test.  The KC end points are loaded before any is used.
+template <int GEOM, bool UNIT, bool CNT, int KC, bool CHECK>
+__device__ __forceinline__ void windows_at(const longlong2* E, int NB, int s, const int (&len)[KC],
+                                           int key0, const WinConsts& kc, Best& best) {
+    const longlong2 e0 = E[s];
+    longlong2 e1[KC];
 #pragma unroll
-        for (int k = 0; k < kC; ++k) len[k] = k0 + k < nd ? lens_smem[k0 + k] : (1 << 29);
-        for (int s = tid; s < NB; s += nthreads) {
-            const longlong2 e0 = E[s];
-            const double c0w = ll_as_d(e0.x), c0y = ll_as_d(e0.y);
-            longlong2 e1[kC];
+    for (int k = 0; k < KC; ++k) {
+        int idx = s + len[k];
+        if (CHECK) {
+            if (GEOM == ATB_GEOM_FIXED && idx > NB) idx -= NB;
+            idx = min(idx, NB);
+        }
+        e1[k] = E[idx];
+    }
 #pragma unroll
-            for (int k = 0; k < kC; ++k) {
-                int idx = s + len[k];
-                if (GEOM == ATB_GEOM_FIXED && idx > NB) idx -= NB;
-                e1[k] = E[min(idx, NB)];
-            }
-#pragma unroll
-            for (int k = 0; k < kC; ++k) {
-                if (k0 + k >= nd) break;  // uniform across the team
-                double dw, dy;
-                bool in_range;
-                if (GEOM == ATB_GEOM_BINNED) {
-                    in_range = s + len[k] <= NB;
-                    dw = ll_as_d(e1[k].x) - c0w;
-                    dy = ll_as_d(e1[k].y) - c0y;
-                } else {
-                    in_range = len[k] < NB;
-                    if (s + len[k] <= NB) {
-                        dw = ll_as_d(e1[k].x) - c0w;
-                        dy = ll_as_d(e1[k].y) - c0y;
-                    } else {
-                        dw = (kc.wtot - c0w) + ll_as_d(e1[k].x);
-                        dy = (kc.ytot - c0y) + ll_as_d(e1[k].y);
-                    }
-                }
-                float num, den;
-                const bool ok = window_eval<GEOM, UNIT>(dw, dy, kc, num, den);
-                if (in_range && ok) best.consider(num, den, s * nd + k0 + k);
+    for (int k = 0; k < KC; ++k) {
+        bool in_range = true;
+        bool wrap = false;
+        if (CHECK) {
+            if (GEOM == ATB_GEOM_BINNED) {
+                in_range = s + len[k] <= NB;
+            } else {
+                in_range = len[k] < NB;
+                wrap = s + len[k] > NB;
             }
         }
+        float num, den;
+        bool ok;
+        if (CNT) {
+            const float c0 = cnt_of(e0.x);
+            float fdw;
+            double dy;
+            if (wrap) {
+                fdw = __fadd_rn(__fsub_rn(kc.fN, c0), cnt_of(e1[k].x));
+                dy = (kc.ytot - ll_as_d(e0.y)) + ll_as_d(e1[k].y);
+            } else {
+                fdw = __fsub_rn(cnt_of(e1[k].x), c0);
+                dy = ll_as_d(e1[k].y) - ll_as_d(e0.y);
+            }
+            ok = window_eval_cnt<GEOM, UNIT>(fdw, dy, kc, num, den);
+        } else {
+            double dw, dy;
+            if (wrap) {
+                dw = (kc.wtot - ll_as_d(e0.x)) + ll_as_d(e1[k].x);
+                dy = (kc.ytot - ll_as_d(e0.y)) + ll_as_d(e1[k].y);
+            } else {
+                dw = ll_as_d(e1[k].x) - ll_as_d(e0.x);
+                dy = ll_as_d(e1[k].y) - ll_as_d(e0.y);
+            }
+            ok = window_eval<GEOM, UNIT>(dw, dy, kc, num, den);
+        }
+        if (in_range && ok) best.consider(num, den, key0 + k);
     }
+}
+
+template <int GEOM, bool UNIT, bool CNT, int KC>
+__device__ __forceinline__ void window_chunk(const longlong2* E, int NB, int nd, int k0,
+                                             const int* lens_smem, int tid, int nthreads,
+                                             const WinConsts& kc, Best& best) {
+    int len[KC];
+    int lmax = 0;
+#pragma unroll
+    for (int k = 0; k < KC; ++k) {
+        len[k] = lens_smem[k0 + k];
+        lmax = max(lmax, len[k]);
+    }
+    // interior starts: s + lmax <= NB (and, with fixed bins, every window
+    // shorter than the period)
+    const int s_end = (GEOM == ATB_GEOM_FIXED && lmax >= NB) ? 0 : NB - lmax + 1;
+    int s = tid;
+    for (; s < s_end; s += nthreads) windows_at<GEOM, UNIT, CNT, KC, false>(E, NB, s, len, s * nd + k0, kc, best);
+    for (; s < NB; s += nthreads) windows_at<GEOM, UNIT, CNT, KC, true>(E, NB, s, len, s * nd + k0, kc, best);
+}
+
+// All windows of one period over starts tid, tid+nthreads, ...  Durations are
+// taken four at a time (then two, then one): the end points of a chunk are
+// loaded together (instruction-level parallelism with few live registers).
+template <int GEOM, bool UNIT, bool CNT>
+__device__ Cand window_search(const longlong2* E, int NB, int nd, const int* lens_smem, int tid,
+                              int nthreads, const WinConsts& kc) {
+    Best best;
+    best.init();
+    int k0 = 0;
+    for (; k0 + 4 <= nd; k0 += 4)
+        window_chunk<GEOM, UNIT, CNT, 4>(E, NB, nd, k0, lens_smem, tid, nthreads, kc, best);
+    if (nd - k0 >= 2) {
+        window_chunk<GEOM, UNIT, CNT, 2>(E, NB, nd, k0, lens_smem, tid, nthreads, kc, best);
+        k0 += 2;
+    }
+    if (nd - k0 >= 1) window_chunk<GEOM, UNIT, CNT, 1>(E, NB, nd, k0, lens_smem, tid, nthreads, kc, best);
     return best.c;
 }
 
@@ -938,10 +1025,15 @@ __device__ void finalize_period(const SearchArgs& a, GroupSmem& gs, const Team& 
     const double IP = gs.IP[g];
 
     if (GEOM == ATB_GEOM_BINNED) {
-        // padding copy, vbls_v42_parity.cu:78-80 (sequential semantics)
-        if (tm.tid == 0) {
-            uint4* R = reinterpret_cast<uint4*>(E);
-            for (int j = 1, ind = NB - a.oversample; j <= a.oversample; ++j, ++ind)
+        // padding copy, vbls_v42_parity.cu:78-80: bins 1..os onto NB-os..NB-1
+        // with sequential semantics; when the two ranges are disjoint
+        // (NB > 2 os) the copies are independent and run in parallel
+        const int os = a.oversample;
+        uint4* R = reinterpret_cast<uint4*>(E);
+        if (NB > 2 * os) {
+            if (tm.tid < os) store_components(R, NB - os + tm.tid, load_components(R, 1 + tm.tid));
+        } else if (tm.tid == 0) {
+            for (int j = 1, ind = NB - os; j <= os; ++j, ++ind)
                 store_components(R, ind, load_components(R, j));
         }
         team_sync(tm);
@@ -954,26 +1046,44 @@ __device__ void finalize_period(const SearchArgs& a, GroupSmem& gs, const Team& 
     }
     team_scan(tm, gs, E, NB + 1, st);
 
-    double wtot, ytot;  // scaled exact totals
+    // scaled exact totals; counting curves: N points of weight qw0s each
+    const bool cnt = st.cnt_win != 0;
+    const double qw0s = ldexp((double)st.qw0, -st.ew);
+    double wtot, ytot;
+    float fN = 0.0f;
     if (GEOM == ATB_GEOM_BINNED) {
         wtot = ldexp((double)st.qw_tot, -st.ew);
         ytot = ldexp((double)st.qy_tot, -st.ey);
+        fN = (float)st.n_cnt;
     } else {
         const longlong2 te = E[NB];
-        wtot = ll_as_d(te.x);
+        if (cnt) {
+            fN = cnt_of(te.x);
+            wtot = (double)fN * qw0s;
+        } else {
+            wtot = ll_as_d(te.x);
+        }
         ytot = ll_as_d(te.y);
     }
+    // exact scaled weight sum of prefix entry i
+    auto pw_at = [&](int i) { return cnt ? (double)cnt_of(E[i].x) * qw0s : ll_as_d(E[i].x); };
     Cand best{-1.0f, 1.0f, 0x7fffffff};
     if (wtot > 0.0) {
         WinConsts kc;
         kc.wtot = wtot;
         kc.ytot = ytot;
-        kc.c1 = (float)(ytot / wtot);
+        kc.c1 = cnt ? (float)(ytot / (double)fN) : (float)(ytot / wtot);
+        kc.fN = fN;
         kc.thr = ldexp(1e-15, st.s_w - st.ew);
+        kc.qw0s = qw0s;
         const int* lens = (GEOM == ATB_GEOM_BINNED) ? gs.dbins : gs.L[tm.id];
         const bool unit = GEOM == ATB_GEOM_FIXED || st.thr_unit;
-        best = unit ? window_search<GEOM, true>(E, NB, nd, lens, tm.tid, tm.nthreads, kc)
-                    : window_search<GEOM, false>(E, NB, nd, lens, tm.tid, tm.nthreads, kc);
+        if (cnt)
+            best = unit ? window_search<GEOM, true, true>(E, NB, nd, lens, tm.tid, tm.nthreads, kc)
+                        : window_search<GEOM, false, true>(E, NB, nd, lens, tm.tid, tm.nthreads, kc);
+        else
+            best = unit ? window_search<GEOM, true, false>(E, NB, nd, lens, tm.tid, tm.nthreads, kc)
+                        : window_search<GEOM, false, false>(E, NB, nd, lens, tm.tid, tm.nthreads, kc);
     }
     best = team_best(tm, gs, best);
 
@@ -987,7 +1097,7 @@ __device__ void finalize_period(const SearchArgs& a, GroupSmem& gs, const Team& 
             double dw, dy;
             if (GEOM == ATB_GEOM_BINNED) {
                 const int dd = gs.dbins[k];
-                dw = ll_as_d(E[s + dd].x) - ll_as_d(E[s].x);
+                dw = pw_at(s + dd) - pw_at(s);
                 dy = ll_as_d(E[s + dd].y) - ll_as_d(E[s].y);
                 const double durv = (double)dd * st.bin_dur;
                 o_dur = (float)durv;
@@ -995,10 +1105,10 @@ __device__ void finalize_period(const SearchArgs& a, GroupSmem& gs, const Team& 
             } else {
                 const int L = gs.L[tm.id][k];
                 if (s + L <= NB) {
-                    dw = ll_as_d(E[s + L].x) - ll_as_d(E[s].x);
+                    dw = pw_at(s + L) - pw_at(s);
                     dy = ll_as_d(E[s + L].y) - ll_as_d(E[s].y);
                 } else {
-                    dw = (wtot - ll_as_d(E[s].x)) + ll_as_d(E[s + L - NB].x);
+                    dw = (wtot - pw_at(s)) + pw_at(s + L - NB);
                     dy = (ytot - ll_as_d(E[s].y)) + ll_as_d(E[s + L - NB].y);
                 }
                 o_dur = (float)gs.dur[k];

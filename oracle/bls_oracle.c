@@ -515,6 +515,30 @@ static inline int eng_window_score(double dw, double dy, const eng_consts* kc, i
     return 1;
 }
 
+/* The same score for curves whose weights are all equal (and n < 2^24):
+ * the engine evaluates it on exact FP32 point counts, W_in = fdw points,
+ * N points in the histogram, c1 = S/N (the score changes by the constant
+ * factor qw0^2 only). */
+static inline int eng_window_score_cnt(float fdw, double dy, float fN, float c1n, int dip_only,
+                                       float* num, float* den)
+{
+    const float fwo = fN - fdw;
+    const float sig = fmaf(c1n, fdw, -(float)dy);
+    if (dip_only && !(sig >= 0.0f)) return 0;
+    *num = sig * sig;
+    *den = fdw * fwo;
+    return 1;
+}
+
+/* Uniform weights with fewer than 2^24 points: windows are scored on counts. */
+static int eng_counting(int64_t n, const int32_t* qw)
+{
+    if (n >= (1LL << 24)) return 0;
+    for (int64_t i = 1; i < n; ++i)
+        if (qw[i] != qw[0]) return 0;
+    return 1;
+}
+
 /* FP64 statistics of the winning window; dw, dy scaled by 2^-ew, 2^-ey */
 static void eng_finalize(double dw, double dy, double wtot, double ytot, int s_w, int s_y,
                          int objective, double* power, double* depth, double* derr)
@@ -572,18 +596,23 @@ int orc_eng_binned(int64_t n, const double* dt, const int32_t* qw, const int32_t
     kc.ytot = y_tot;
     kc.c1 = w_tot > 0.0 ? (float)(y_tot / w_tot) : 0.0f;
     kc.thr = ldexp(1e-15, st->s_w - ew);
+    const int counting = eng_counting(n, qw);
+    const float fN = (float)n;
+    const float c1n = (float)(y_tot / (double)n);
 
     int err = ORC_OK;
     set_threads(nthreads);
 #pragma omp parallel
     {
-        int64_t* hw = (int64_t*)malloc(sizeof(int64_t) * 2 * (size_t)cap);
+        int64_t* hw = (int64_t*)malloc(sizeof(int64_t) * 3 * (size_t)cap);
         double* cw = (double*)malloc(sizeof(double) * 2 * (size_t)cap);
-        if (!hw || !cw) {
+        float* cc = (float*)malloc(sizeof(float) * (size_t)cap);
+        if (!hw || !cw || !cc) {
 #pragma omp atomic write
             err = ORC_ENOMEM;
         } else {
             int64_t* hy = hw + cap;
+            int64_t* hc = hw + 2 * cap;
             double* cy = cw + cap;
 #pragma omp for schedule(dynamic, 4)
             for (int64_t p = 0; p < np; ++p) {
@@ -593,22 +622,27 @@ int orc_eng_binned(int64_t n, const double* dt, const int32_t* qw, const int32_t
                 if (max_bins > 0 && n_bins >= max_bins) n_bins = max_bins - 1;
                 memset(hw, 0, sizeof(int64_t) * (size_t)(n_bins + 1));
                 memset(hy, 0, sizeof(int64_t) * (size_t)(n_bins + 1));
+                memset(hc, 0, sizeof(int64_t) * (size_t)(n_bins + 1));
                 for (int64_t i = 0; i < n; ++i) {
                     const int ind = eng_fold_binned(dt[i], period, inv_period, inv_bin_dur, n_bins);
                     if (point_bins) point_bins[p * n + i] = ind;
                     hw[ind] += qw[i];
                     hy[ind] += qy[i];
+                    hc[ind] += 1;
                 }
                 for (int j = 1, ind = n_bins - oversample; j <= oversample; ++j, ++ind) {
                     hw[ind] = hw[j];
                     hy[ind] = hy[j];
+                    hc[ind] = hc[j];
                 }
-                int64_t aw = 0, ay = 0;
+                int64_t aw = 0, ay = 0, ac = 0;
                 for (int j = 0; j <= n_bins; ++j) {
                     aw += hw[j];
                     ay += hy[j];
+                    ac += hc[j];
                     cw[j] = ldexp((double)aw, -ew);
                     cy[j] = ldexp((double)ay, -ey);
+                    cc[j] = (float)ac;
                 }
                 eng_cand best = {-1.0f, 1.0f, INT32_MAX};
                 for (int s = 0; s < n_bins; ++s) {
@@ -619,7 +653,13 @@ int orc_eng_binned(int64_t n, const double* dt, const int32_t* qw, const int32_t
                         const double dy = cy[s + d] - cy[s];
                         if (dw < kc.thr || (w_tot - dw) < kc.thr) continue;
                         float num, den;
-                        if (!eng_window_score(dw, dy, &kc, 1, &num, &den)) continue;
+                        if (counting) {
+                            if (!eng_window_score_cnt(cc[s + d] - cc[s], dy, fN, c1n, 1, &num,
+                                                      &den))
+                                continue;
+                        } else if (!eng_window_score(dw, dy, &kc, 1, &num, &den)) {
+                            continue;
+                        }
                         eng_consider(&best, num, den, s * nd + k);
                     }
                 }
@@ -645,6 +685,7 @@ int orc_eng_binned(int64_t n, const double* dt, const int32_t* qw, const int32_t
         }
         free(hw);
         free(cw);
+        free(cc);
     }
     return err;
 }
@@ -659,38 +700,47 @@ int orc_eng_fixed(int64_t n, const double* dt, const int32_t* qw, const int32_t*
     int err = ORC_OK;
     const double nbd = (double)n_bins;
     const int ew = exp_above((double)st->qw_tot), ey = exp_above((double)st->qy_abs);
+    const int counting = eng_counting(n, qw);
     set_threads(nthreads);
 #pragma omp parallel
     {
-        int64_t* hw = (int64_t*)malloc(sizeof(int64_t) * 2 * (size_t)(n_bins + 1));
+        int64_t* hw = (int64_t*)malloc(sizeof(int64_t) * 3 * (size_t)(n_bins + 1));
         double* cw = (double*)malloc(sizeof(double) * 2 * (size_t)(n_bins + 1));
-        if (!hw || !cw) {
+        float* cc = (float*)malloc(sizeof(float) * (size_t)(n_bins + 1));
+        if (!hw || !cw || !cc) {
 #pragma omp atomic write
             err = ORC_ENOMEM;
         } else {
             int64_t* hy = hw + (n_bins + 1);
+            int64_t* hc = hw + 2 * (n_bins + 1);
             double* cy = cw + (n_bins + 1);
 #pragma omp for schedule(dynamic, 4)
             for (int64_t p = 0; p < np; ++p) {
                 const double inv_p = 1.0 / periods[p];
                 memset(hw, 0, sizeof(int64_t) * (size_t)(n_bins + 1));
                 memset(hy, 0, sizeof(int64_t) * (size_t)(n_bins + 1));
+                memset(hc, 0, sizeof(int64_t) * (size_t)(n_bins + 1));
                 for (int64_t i = 0; i < n; ++i) {
                     const int slot = eng_fold_fixed(dt[i], inv_p, nbd, n_bins);
                     if (point_bins) point_bins[p * n + i] = slot;
                     if (slot >= 0) {
                         hw[slot] += qw[i];
                         hy[slot] += qy[i];
+                        hc[slot] += 1;
                     }
                 }
-                int64_t aw = 0, ay = 0;
+                int64_t aw = 0, ay = 0, ac = 0;
                 for (int j = 0; j <= n_bins; ++j) {
                     aw += hw[j];
                     ay += hy[j];
+                    ac += hc[j];
                     cw[j] = ldexp((double)aw, -ew);
                     cy[j] = ldexp((double)ay, -ey);
+                    cc[j] = (float)ac;
                 }
                 const double w_tot = cw[n_bins], y_tot = cy[n_bins];
+                const float fN = cc[n_bins];
+                const float c1n = fN > 0.0f ? (float)(y_tot / (double)fN) : 0.0f;
                 eng_cand best = {-1.0f, 1.0f, INT32_MAX};
                 if (w_tot > 0.0) {
                     eng_consts kc;
@@ -704,16 +754,22 @@ int orc_eng_fixed(int64_t n, const double* dt, const int32_t* qw, const int32_t*
                             if (L < 1) L = 1;
                             if (L >= n_bins) continue;
                             double dw, dy;
+                            float fdw;
                             if (s + L <= n_bins) {
                                 dw = cw[s + L] - cw[s];
                                 dy = cy[s + L] - cy[s];
+                                fdw = cc[s + L] - cc[s];
                             } else {
                                 dw = (w_tot - cw[s]) + cw[s + L - n_bins];
                                 dy = (y_tot - cy[s]) + cy[s + L - n_bins];
+                                fdw = (fN - cc[s]) + cc[s + L - n_bins];
                             }
                             if (!(dw > 0.0 && dw < w_tot)) continue;
                             float num, den;
-                            eng_window_score(dw, dy, &kc, 0, &num, &den);
+                            if (counting)
+                                eng_window_score_cnt(fdw, dy, fN, c1n, 0, &num, &den);
+                            else
+                                eng_window_score(dw, dy, &kc, 0, &num, &den);
                             eng_consider(&best, num, den, s * nd + k);
                         }
                     }
@@ -748,6 +804,7 @@ int orc_eng_fixed(int64_t n, const double* dt, const int32_t* qw, const int32_t*
         }
         free(hw);
         free(cw);
+        free(cc);
     }
     return err;
 }
