@@ -862,59 +862,59 @@ struct WinConsts {
 // Weighted curves pass exact scaled FP64 weight sums (dw); counting curves
 // pass the exact FP32 point count of the window (fdw) and use N and S/N in
 // place of W and S/W (the same score up to the constant factor qw0s^2).
+// The dip-only rule of the astropy-binned geometry is carried by the sign of
+// num = sigma*|sigma|: a window with sigma < 0 has num < 0 and never passes
+// the filter num >= lim*den (lim >= 0, den > 0), and for sigma >= 0 num is
+// sigma^2.  den > 0 is exactly "W_in > 0 and W_out > 0" (both are
+// non-negative).
 template <int GEOM, bool UNIT>
 __device__ __forceinline__ bool window_eval(double dw, double dy, const WinConsts& kc, float& num,
                                             float& den) {
     const double wo = kc.wtot - dw;
     const float fdw = __double2float_rn(dw);
     const float fwo = __double2float_rn(wo);
-    bool ok;
-    if (UNIT) {
-        ok = fdw > 0.0f && fwo > 0.0f;  // exact: dw, wo are scaled integers and thr < 1 unit
-    } else {
-        ok = !(dw < kc.thr || wo < kc.thr);
-    }
     const float sig = __fmaf_rn(kc.c1, fdw, -__double2float_rn(dy));
-    if (GEOM == ATB_GEOM_BINNED) ok = ok && (sig >= 0.0f);
-    num = __fmul_rn(sig, sig);
+    num = __fmul_rn(sig, GEOM == ATB_GEOM_BINNED ? fabsf(sig) : sig);
     den = __fmul_rn(fdw, fwo);
-    return ok;
+    if (UNIT) return den > 0.0f;  // exact: dw, wo are scaled integers and thr < 1 unit
+    return !(dw < kc.thr || wo < kc.thr);
 }
 
 template <int GEOM, bool UNIT>
 __device__ __forceinline__ bool window_eval_cnt(float fdw, double dy, const WinConsts& kc,
                                                 float& num, float& den) {
     const float fwo = __fsub_rn(kc.fN, fdw);  // exact: integers below 2^24
-    bool ok;
-    if (UNIT) {
-        ok = fdw > 0.0f && fwo > 0.0f;
-    } else {
-        ok = !((double)fdw * kc.qw0s < kc.thr || (double)fwo * kc.qw0s < kc.thr);
-    }
     const float sig = __fmaf_rn(kc.c1, fdw, -__double2float_rn(dy));
-    if (GEOM == ATB_GEOM_BINNED) ok = ok && (sig >= 0.0f);
-    num = __fmul_rn(sig, sig);
+    num = __fmul_rn(sig, GEOM == ATB_GEOM_BINNED ? fabsf(sig) : sig);
     den = __fmul_rn(fdw, fwo);
-    return ok;
+    if (UNIT) return den > 0.0f;
+    return !((double)fdw * kc.qw0s < kc.thr || (double)fwo * kc.qw0s < kc.thr);
 }
 
-// Running best with a division-free pre-filter: `lim` is a lower bound of the
-// best ratio (rounded down by 2^-20), so num < lim*den can never win the exact
-// comparison and skips it.
+// Running best with a division-free pre-filter: `lim` (>= 0) is a lower bound
+// of a ratio some window of the period reaches (rounded down by 2^-20), so
+// num < lim*den can never win the exact comparison and is skipped.  share()
+// gives every lane of the warp the largest lim of the warp: a window below
+// another lane's best cannot be the period's best, and exact ties still pass
+// the filter, so the lowest-key rule is unaffected.
 struct Best {
     Cand c;
     float lim;
     __device__ __forceinline__ void init() {
         c = Cand{-1.0f, 1.0f, 0x7fffffff};
-        lim = -2.0f;
+        lim = 0.0f;
     }
     __device__ __forceinline__ void consider(float num, float den, int key) {
         if (num >= __fmul_rn(lim, den) && cand_better(num, den, key, c.num, c.den, c.key)) {
             c.num = num;
             c.den = den;
             c.key = key;
-            lim = __fmul_rn(__fdiv_rn(num, den), 0.99999904632568359375f);  // 1 - 2^-20
+            lim = fmaxf(lim, __fmul_rn(__fdiv_rn(num, den), 0.99999904632568359375f));  // 1 - 2^-20
         }
+    }
+    // non-negative floats order like their bit patterns; every lane must call it
+    __device__ __forceinline__ void share() {
+        lim = __int_as_float(__reduce_max_sync(0xffffffffu, __float_as_int(lim)));
     }
 };
 
@@ -925,7 +925,8 @@ __device__ __forceinline__ float cnt_of(long long x) { return __int_as_float((in
 // wrap and no range test.  The KC end points are loaded before any is used.
 template <int GEOM, bool UNIT, bool CNT, int KC, bool CHECK>
 __device__ __forceinline__ void windows_at(const longlong2* E, int NB, int s, const int (&len)[KC],
-                                           int key0, const WinConsts& kc, Best& best) {
+                                           const WinConsts& kc, float (&num)[KC], float (&den)[KC],
+                                           bool (&ok)[KC]) {
     const longlong2 e0 = E[s];
     longlong2 e1[KC];
 #pragma unroll
@@ -949,8 +950,7 @@ __device__ __forceinline__ void windows_at(const longlong2* E, int NB, int s, co
                 wrap = s + len[k] > NB;
             }
         }
-        float num, den;
-        bool ok;
+        bool okk;
         if (CNT) {
             const float c0 = cnt_of(e0.x);
             float fdw;
@@ -962,7 +962,7 @@ __device__ __forceinline__ void windows_at(const longlong2* E, int NB, int s, co
                 fdw = __fsub_rn(cnt_of(e1[k].x), c0);
                 dy = ll_as_d(e1[k].y) - ll_as_d(e0.y);
             }
-            ok = window_eval_cnt<GEOM, UNIT>(fdw, dy, kc, num, den);
+            okk = window_eval_cnt<GEOM, UNIT>(fdw, dy, kc, num[k], den[k]);
         } else {
             double dw, dy;
             if (wrap) {
@@ -972,9 +972,30 @@ __device__ __forceinline__ void windows_at(const longlong2* E, int NB, int s, co
                 dw = ll_as_d(e1[k].x) - ll_as_d(e0.x);
                 dy = ll_as_d(e1[k].y) - ll_as_d(e0.y);
             }
-            ok = window_eval<GEOM, UNIT>(dw, dy, kc, num, den);
+            okk = window_eval<GEOM, UNIT>(dw, dy, kc, num[k], den[k]);
         }
-        if (in_range && ok) best.consider(num, den, key0 + k);
+        ok[k] = in_range && okk;
+    }
+}
+
+// The division-free filter for the KC windows of one step of the warp; the
+// exact comparison runs only in the (rare) steps where some lane has a
+// window passing it.  Every lane of the warp must call it.
+template <int KC>
+__device__ __forceinline__ void window_filter(const float (&num)[KC], const float (&den)[KC],
+                                              const bool (&ok)[KC], int key0, Best& best) {
+    bool pass[KC];
+    bool any = false;
+#pragma unroll
+    for (int k = 0; k < KC; ++k) {
+        pass[k] = ok[k] && num[k] >= __fmul_rn(best.lim, den[k]);
+        any = any || pass[k];
+    }
+    if (__any_sync(0xffffffffu, any)) {
+#pragma unroll
+        for (int k = 0; k < KC; ++k)
+            if (pass[k]) best.consider(num[k], den[k], key0 + k);
+        best.share();
     }
 }
 
@@ -992,9 +1013,37 @@ __device__ __forceinline__ void window_chunk(const longlong2* E, int NB, int nd,
     // interior starts: s + lmax <= NB (and, with fixed bins, every window
     // shorter than the period)
     const int s_end = (GEOM == ATB_GEOM_FIXED && lmax >= NB) ? 0 : NB - lmax + 1;
-    int s = tid;
-    for (; s < s_end; s += nthreads) windows_at<GEOM, UNIT, CNT, KC, false>(E, NB, s, len, s * nd + k0, kc, best);
-    for (; s < NB; s += nthreads) windows_at<GEOM, UNIT, CNT, KC, true>(E, NB, s, len, s * nd + k0, kc, best);
+    // warp-uniform trip count (lanes past NB skip the body), so that the
+    // warp can share its filter bound after every step
+    const int lane = tid & 31;
+    int s0 = tid - lane;
+    // interior steps (every lane's start is interior): no divergence
+    for (; s0 + 31 < s_end; s0 += nthreads) {
+        const int s = s0 + lane;
+        float num[KC], den[KC];
+        bool ok[KC];
+        windows_at<GEOM, UNIT, CNT, KC, false>(E, NB, s, len, kc, num, den, ok);
+        window_filter<KC>(num, den, ok, s * nd + k0, best);
+    }
+    // the remaining steps
+    for (; s0 < NB; s0 += nthreads) {
+        const int s = s0 + lane;
+        float num[KC], den[KC];
+        bool ok[KC];
+        if (s < s_end) {
+            windows_at<GEOM, UNIT, CNT, KC, false>(E, NB, s, len, kc, num, den, ok);
+        } else if (s < NB) {
+            windows_at<GEOM, UNIT, CNT, KC, true>(E, NB, s, len, kc, num, den, ok);
+        } else {
+#pragma unroll
+            for (int k = 0; k < KC; ++k) {
+                num[k] = 0.0f;
+                den[k] = 1.0f;
+                ok[k] = false;
+            }
+        }
+        window_filter<KC>(num, den, ok, s * nd + k0, best);
+    }
 }
 
 // All windows of one period over starts tid, tid+nthreads, ...  Durations are
