@@ -503,9 +503,10 @@ __device__ __forceinline__ void red_shared_u32(unsigned addr, unsigned v) {
 // Histogram entry of slot s: four 32-bit words -- weight sums split at
 // `lobits` (x, y; x = point count when weights are uniform) and flux sums
 // split the same way (z, w).  Component c is stored in word c ^ rot(s),
-// rot(s) = (s >> 3) & 3, so that for a fixed component consecutive slots
-// cycle through all 32 banks (a plain 16-byte layout would use only 8).
-__device__ __forceinline__ unsigned slot_rot(int s) { return ((unsigned)s >> 3) & 3u; }
+// rot(s) = ((s - 1) >> 3) & 3, so that for a fixed component consecutive
+// slots cycle through all 32 banks (a plain 16-byte layout would use only 8).
+// The fold addresses slots as 1 + t (t = slot - 1), hence the offset.
+__device__ __forceinline__ unsigned slot_rot(int s) { return ((unsigned)(s - 1) >> 3) & 3u; }
 
 __device__ __forceinline__ uint4 load_components(const uint4* H, int s) {
     uint4 e = H[s];
@@ -553,10 +554,8 @@ __device__ __forceinline__ void team_sync(const Team& tm) {
 struct GroupSmem {
     double tP[kTileP];   // the tile's periods
     int tNB[kTileP];     // and their bin counts
-    double P[kMaxG];
-    double IP[kMaxG];
-    int NB[kMaxG];
-    int base[kMaxG];
+    double2 PIP[kMaxG];  // (P, 1/P) of each period of the group
+    int2 NBB[kMaxG];     // (bin count, histogram offset) of each period
     long long slot[kMaxG];
     int dbins[kMaxDur];
     double dur[kMaxDur];
@@ -574,18 +573,21 @@ struct GroupSmem {
     int safe_floor;  // |dt / P| < 2^50 over the group: floor via floor_magic
 };
 
-// Histogram slots of one thread's kR points for one period.
+// Histogram slots of one thread's kR points for one period, returned as
+// t = slot - 1.
 //   astropy-binned (vbls_v42_parity.cu:65-70): ph = fma(-P, floor(d*IP), d),
-//     slot = min(int(ph*inv_bin_dur) + 1, n_bins)
-//   fixed bins (bls.cu:52-62): ph = d*IP - floor(d*IP), b = int(ph*n_bins),
-//     slot = b + 1, or the trash slot n_bins + 1 for b outside [0, n_bins)
+//     slot = min(int(ph*inv_bin_dur) + 1, n_bins), i.e. t = min(max(int, 0), n_bins - 1)
+//   fixed bins (bls.cu:52-62): ph = d*IP - floor(d*IP) in [0, 1), b = int(ph*n_bins)
+//     in [0, n_bins]; slot = b + 1, where b = n_bins (a product rounded up to
+//     n_bins) is the trash slot n_bins + 1 that no window reads.  The unsigned
+//     minimum keeps non-finite inputs (flagged by the staging) in the trash slot.
 // floor and trunc are computed with exact
 // magic-constant additions, and when the points are time-ordered and the first
 // and last share the cycle index k = floor(d*IP), every point between them has
 // the same k (rounded multiplication and floor are monotone), so k is reused.
 template <int GEOM>
 __device__ __forceinline__ void fold_slots(const double (&d)[kR], bool sorted, bool safe_floor,
-                                           double P, double IP, double ibd, int NB, int (&sl)[kR]) {
+                                           double P, double IP, double ibd, int NB, int (&t)[kR]) {
     double k0, k7;
     const double m0 = d[0] * IP, m7 = d[kR - 1] * IP;
     if (safe_floor) {
@@ -601,12 +603,10 @@ __device__ __forceinline__ void fold_slots(const double (&d)[kR], bool sorted, b
         for (int j = 0; j < kR; ++j) {
             if (GEOM == ATB_GEOM_BINNED) {
                 const double ph = fma(-P, k0, d[j]);
-                const int ind = max(trunc_magic(ph * ibd), 0) + 1;
-                sl[j] = min(ind, NB);
+                t[j] = min(max(trunc_magic(ph * ibd), 0), NB - 1);
             } else {
                 const double m = (j == 0) ? m0 : (j == kR - 1 ? m7 : d[j] * IP);
-                const int b = trunc_magic((m - k0) * nbd);
-                sl[j] = (b < NB) ? b + 1 : NB + 1;
+                t[j] = (int)min((unsigned)trunc_magic((m - k0) * nbd), (unsigned)NB);
             }
         }
     } else {
@@ -616,32 +616,32 @@ __device__ __forceinline__ void fold_slots(const double (&d)[kR], bool sorted, b
             const double k = safe_floor ? floor_magic(m) : floor(m);
             if (GEOM == ATB_GEOM_BINNED) {
                 const double ph = fma(-P, k, d[j]);
-                const int ind = max(trunc_magic(ph * ibd), 0) + 1;
-                sl[j] = min(ind, NB);
+                t[j] = min(max(trunc_magic(ph * ibd), 0), NB - 1);
             } else {
-                const int b = trunc_magic((m - k) * nbd);
-                sl[j] = (b >= 0 && b < NB) ? b + 1 : NB + 1;
+                t[j] = (int)min((unsigned)trunc_magic((m - k) * nbd), (unsigned)NB);
             }
         }
     }
 }
 
-// fold every staged point of the curve into the group's histograms
-// Add one point's words to histogram entry `slot` (component c of the entry
-// lives at word c ^ rot(slot)).  MODE selects the layout (kPack*); words a..d
-// are the point's components x, y, z, w (unused ones are ignored).
+// Add one point's words to histogram slot 1 + t (component c of the entry
+// lives at word c ^ rot(1 + t)); `base1` is the shared-memory address of slot 1
+// (H1 the pointer to it for global histograms).  MODE selects the layout
+// (kPack*); words a..d are the point's components x, y, z, w (unused ones are
+// ignored).
 template <bool GLOB, int MODE>
-__device__ __forceinline__ void hist_add_point(uint4* H, int slot, unsigned a, unsigned b,
-                                               unsigned c, unsigned d) {
-    const unsigned r = slot_rot(slot);
+__device__ __forceinline__ void hist_add_point(unsigned base1, uint4* H1, int t, unsigned a,
+                                               unsigned b, unsigned c, unsigned d) {
     if (GLOB) {
-        unsigned* e = reinterpret_cast<unsigned*>(H + slot);
+        const unsigned r = ((unsigned)t >> 3) & 3u;
+        unsigned* e = reinterpret_cast<unsigned*>(H1 + t);
         atomicAdd(e + (0u ^ r), a);
         if (MODE == kPackSplit) atomicAdd(e + (1u ^ r), b);
         atomicAdd(e + (2u ^ r), c);
         if (MODE != kPackTight) atomicAdd(e + (3u ^ r), d);
     } else {
-        const unsigned ad = (unsigned)__cvta_generic_to_shared(H + slot) | (r << 2);
+        // base1 + 16 t has four low zero bits; rot(1 + t) << 2 = (t >> 1) & 12
+        const unsigned ad = (base1 + 16u * (unsigned)t) | (((unsigned)t >> 1) & 12u);
         red_shared_u32(ad, a);
         if (MODE == kPackSplit) red_shared_u32(ad ^ 4u, b);
         red_shared_u32(ad ^ 8u, c);
@@ -700,12 +700,15 @@ __device__ void fold_group(const SearchArgs& a, const GroupSmem& gs, uint4* H, l
             }
         }
         for (int g = 0; g < G; ++g) {
-            const int NB = gs.NB[g];
-            int sl[kR];
-            fold_slots<GEOM>(d, sorted, safe, gs.P[g], gs.IP[g], st.inv_bin_dur, NB, sl);
-            uint4* Hg = H + gs.base[g];
+            const double2 pip = gs.PIP[g];
+            const int2 nbb = gs.NBB[g];
+            int t[kR];
+            fold_slots<GEOM>(d, sorted, safe, pip.x, pip.y, st.inv_bin_dur, nbb.x, t);
+            uint4* H1 = H + nbb.y + 1;
+            const unsigned base1 = GLOB ? 0u : (unsigned)__cvta_generic_to_shared(H1);
 #pragma unroll
-            for (int j = 0; j < kR; ++j) hist_add_point<GLOB, MODE>(Hg, sl[j], wa[j], wb[j], wc[j], wd[j]);
+            for (int j = 0; j < kR; ++j)
+                hist_add_point<GLOB, MODE>(base1, H1, t[j], wa[j], wb[j], wc[j], wd[j]);
         }
     }
 }
@@ -1068,10 +1071,10 @@ __device__ Cand window_search(const longlong2* E, int NB, int nd, const int* len
 template <int GEOM>
 __device__ void finalize_period(const SearchArgs& a, GroupSmem& gs, const Team& tm, longlong2* H,
                                 int g, const CurveStat& st, int nd) {
-    longlong2* E = H + gs.base[g];
-    const int NB = gs.NB[g];
-    const double P = gs.P[g];
-    const double IP = gs.IP[g];
+    longlong2* E = H + gs.NBB[g].y;
+    const int NB = gs.NBB[g].x;
+    const double P = gs.PIP[g].x;
+    const double IP = gs.PIP[g].y;
 
     if (GEOM == ATB_GEOM_BINNED) {
         // padding copy, vbls_v42_parity.cu:78-80: bins 1..os onto NB-os..NB-1
@@ -1275,11 +1278,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) search_kernel(const Search
                     const int NB = gs.tNB[li];
                     const int need = NB + 2;
                     if (g > 0 && base + need > a.cap) break;
-                    gs.P[g] = P;
-                    gs.IP[g] = 1.0 / P;
-                    ipmax = max(ipmax, gs.IP[g]);
-                    gs.NB[g] = NB;
-                    gs.base[g] = base;
+                    const double IP = 1.0 / P;
+                    ipmax = max(ipmax, IP);
+                    gs.PIP[g] = make_double2(P, IP);
+                    gs.NBB[g] = make_int2(NB, base);
                     gs.slot[g] = obeg + p;
                     base += need;
                     ++g;
@@ -1351,11 +1353,11 @@ __global__ void debug_fold_kernel(const double* sdt, long long n, const CurveSta
         for (int j = 0; j + 1 < kR; ++j) sorted = sorted && (d[j] <= d[j + 1]);
         const double IP = 1.0 / P;
         const bool safe = st.dt_absmax * IP < 1.0e15;
-        int sl[kR];
-        fold_slots<GEOM>(d, sorted, safe, P, IP, st.inv_bin_dur, NB, sl);
+        int t[kR];
+        fold_slots<GEOM>(d, sorted, safe, P, IP, st.inv_bin_dur, NB, t);
 #pragma unroll
         for (int j = 0; j < kR; ++j)
-            if (ch * kR + j < n) out[p * n + ch * kR + j] = sl[j];
+            if (ch * kR + j < n) out[p * n + ch * kR + j] = t[j] + 1;
     }
 }
 
