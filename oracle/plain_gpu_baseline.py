@@ -1,0 +1,113 @@
+"""Timing of the plain one-call-per-curve GPU path (the denominator of the
+batched-engine speed-up) beside the engine, on curves of the uniform-batch
+workload (2-min cadence, 15 000 points, 5 000 log-spaced periods 0.5-13.7 d,
+6 durations 0.04-0.20 d).
+
+TEST INFRASTRUCTURE: runs the reference's own kernels (compiled from source
+into oracle/_ref by oracle/Makefile) through oracle.ref_kernels, whose host
+code restates the reference's CuPy wrappers, one curve per call with the host
+prologue, host-to-device copies and result copies included, as the reference
+does:
+
+* fast path   search/gpu_bls.py:42-144, bls.cu with SCALAR_T=double, N_TILE=4
+              (and the float build, the reference's default dtype)
+* parity path search/v42_parity.py:27-107, vbls_v42_parity.cu FP64, one curve
+              per launch, max_bins large enough for every period of the grid
+
+and, for comparison, the engine on the same curves: batched (inputs resident),
+and one curve per BoxLeastSquaresGPU.power call.  Prints one JSON object.
+
+    python oracle/plain_gpu_baseline.py [--curves 4096] [--sample 32]
+"""
+import argparse
+import json
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+
+import torch  # noqa: E402
+
+import recipes as R  # noqa: E402
+from astro_transit_gpu_b200.api import BoxLeastSquaresGPU  # noqa: E402
+from astro_transit_gpu_b200.engine import BatchSession, BLSEngine, SearchConfig  # noqa: E402
+from oracle.ref_kernels import RefKernels  # noqa: E402
+
+DURATIONS = np.array([0.04, 0.06, 0.08, 0.12, 0.16, 0.20])
+
+
+def per_curve_rate(fn, n):
+    fn(0)  # warm-up (module load, allocator)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in range(n):
+        fn(i)
+    torch.cuda.synchronize()
+    return n / (time.perf_counter() - t0)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--curves", type=int, default=4096, help="batched engine batch size")
+    ap.add_argument("--sample", type=int, default=32, help="curves timed one call at a time")
+    ap.add_argument("--v42-sample", type=int, default=4)
+    args = ap.parse_args()
+
+    nc = max(args.curves, args.sample)
+    t, y, dy, _ = R.uniform_batch(n_curves=nc, n=15000, seed=1000)
+    periods = R.c0_periods(5000)
+    rk = RefKernels()
+    out = {"workload": "uniform batch curves: 15000 points, 5000 log-spaced periods 0.5-13.7 d, "
+                       "6 durations 0.04-0.20 d", "sample_curves": args.sample}
+
+    # reference fast path (fixed 200 bins), one curve per call
+    for dt, key in ((np.float64, "ref_bls_fp64_per_curve"), (np.float32, "ref_bls_fp32_per_curve")):
+        out[key] = per_curve_rate(
+            lambda i: rk.run_gpu_bls(t[i], y[i], periods, DURATIONS, flux_err=dy[i], n_bins=200,
+                                     dtype=dt), args.sample)
+    # reference parity path (astropy-binned), one curve per launch
+    nb_max = int(np.ceil(periods.max() / (DURATIONS.min() / 10))) + 10
+    out["ref_v42_fp64_per_curve"] = per_curve_rate(
+        lambda i: rk.run_vbls_exact_parity(t[i], y[i].reshape(1, -1), periods, DURATIONS,
+                                           weights_matrix=(1.0 / dy[i].astype(np.float64) ** 2)
+                                           .reshape(1, -1), oversample=10, max_bins=nb_max + 2,
+                                           dtype=np.float64), args.v42_sample)
+    out["v42_sample_curves"] = args.v42_sample
+
+    # the engine, one curve per public API call (host arrays in, results out)
+    for method, key, kw in (("fast", "engine_fast_per_call", {"n_bins": 200}),
+                            ("parity", "engine_parity_per_call",
+                             {"objective": "likelihood"})):
+        out[key] = per_curve_rate(
+            lambda i: BoxLeastSquaresGPU(t[i], y[i], dy[i]).power(periods, DURATIONS,
+                                                                  method=method, **kw),
+            args.sample)
+
+    # the engine batched, inputs resident (device time of the search)
+    eng = BLSEngine.get(0)
+    w = (1.0 / dy.astype(np.float64) ** 2).astype(np.float32)
+    for cfg, key in ((SearchConfig("fast", n_bins=200), "engine_fast_batched"),
+                     (SearchConfig("parity", objective="likelihood"), "engine_parity_batched")):
+        sess = BatchSession(eng, np.arange(args.curves + 1) * 15000, periods, DURATIONS, cfg,
+                            weighted=True)
+        sess.load(t[:args.curves], y[:args.curves], w[:args.curves])
+        sess.run()
+        torch.cuda.synchronize()
+        ms = min(sess.plan.profile()["search"] for _ in range(3))
+        out[key] = args.curves / (ms * 1e-3)
+        del sess
+    out["speedup_fast_batched_vs_ref_fp64_per_curve"] = (
+        out["engine_fast_batched"] / out["ref_bls_fp64_per_curve"])
+    out["speedup_parity_batched_vs_ref_v42_fp64_per_curve"] = (
+        out["engine_parity_batched"] / out["ref_v42_fp64_per_curve"])
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()
