@@ -235,12 +235,10 @@ def main():
             dist.barrier()
         torch.cuda.synchronize(dev)
 
+    from astro_transit_gpu_b200.sharding import max_over_ranks as _max_over_ranks
+
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        v = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(v, op=dist.ReduceOp.MAX)
-        return float(v.item())
+        return _max_over_ranks(x, device=dev)
 
     for _ in range(args.warmup):
         plan.execute(stream)
