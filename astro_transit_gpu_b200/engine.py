@@ -403,6 +403,8 @@ class BatchSession:
         self.host_out = {k: torch.empty(v.shape, dtype=v.dtype).pin_memory()
                          for k, v in self.outputs.items()}
         self.plan = engine.plan(self.batch, config, self.outputs)
+        self.step_graph = None    # H2D copies + search + D2H copies
+        self.search_graph = None  # the search alone (inputs resident)
 
     @property
     def h2d_bytes(self) -> int:
@@ -419,17 +421,51 @@ class BatchSession:
         if "w" in self.host:
             self.host["w"].numpy()[:] = np.ravel(w)
 
+    def _enqueue_step(self, s: torch.cuda.Stream) -> None:
+        for k, v in self.host.items():
+            self.dev_in[k].copy_(v, non_blocking=True)
+        self.plan.execute(s)
+        for k, v in self.outputs.items():
+            self.host_out[k].copy_(v, non_blocking=True)
+
+    def capture(self) -> None:
+        """Record the session's step (input copies, the search's kernels, output
+        copies) and the search alone into two CUDA graphs; afterwards
+        :meth:`run` and :meth:`search` replay them with one launch each.  The
+        graphs read the pinned host buffers, so :meth:`load` between replays
+        feeds new light curves of the same shape."""
+        dev = self.batch.device
+        torch.cuda.synchronize(dev)
+        side = torch.cuda.Stream(dev)
+        g_step, g_search = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g_step, stream=side):
+            self._enqueue_step(side)
+        with torch.cuda.graph(g_search, stream=side):
+            self.plan.execute(side)
+        torch.cuda.synchronize(dev)
+        self.step_graph, self.search_graph = g_step, g_search
+
     def run(self, stream: Optional[torch.cuda.Stream] = None) -> Dict[str, torch.Tensor]:
-        """Enqueue H2D inputs, the search and D2H outputs on `stream`; the pinned
-        host outputs are valid once the stream has synchronised."""
+        """Enqueue H2D inputs, the search and D2H outputs on `stream` (one graph
+        launch after :meth:`capture`); the pinned host outputs are valid once
+        the stream has synchronised."""
         s = stream if stream is not None else torch.cuda.current_stream(self.batch.device)
         with torch.cuda.stream(s):
-            for k, v in self.host.items():
-                self.dev_in[k].copy_(v, non_blocking=True)
-            self.plan.execute(s)
-            for k, v in self.outputs.items():
-                self.host_out[k].copy_(v, non_blocking=True)
+            if self.step_graph is not None:
+                self.step_graph.replay()
+            else:
+                self._enqueue_step(s)
         return self.host_out
+
+    def search(self, stream: Optional[torch.cuda.Stream] = None) -> None:
+        """Enqueue the search on the resident inputs (graph replay after
+        :meth:`capture`)."""
+        s = stream if stream is not None else torch.cuda.current_stream(self.batch.device)
+        if self.search_graph is not None:
+            with torch.cuda.stream(s):
+                self.search_graph.replay()
+        else:
+            self.plan.execute(s)
 
 
 def _grid_arrays(g, nc):
