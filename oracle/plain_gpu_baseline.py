@@ -57,7 +57,12 @@ def main():
     ap.add_argument("--curves", type=int, default=4096, help="batched engine batch size")
     ap.add_argument("--sample", type=int, default=32, help="curves timed one call at a time")
     ap.add_argument("--v42-sample", type=int, default=4)
+    ap.add_argument("--workload", default="uniform", choices=["uniform", "mixed"],
+                    help="mixed: the uneven batch (fast method only, reference bls.cu vs "
+                         "the engine batched)")
     args = ap.parse_args()
+    if args.workload == "mixed":
+        return mixed(args)
 
     nc = max(args.curves, args.sample)
     t, y, dy, _ = R.uniform_batch(n_curves=nc, n=15000, seed=1000)
@@ -106,6 +111,49 @@ def main():
         out["engine_fast_batched"] / out["ref_bls_fp64_per_curve"])
     out["speedup_parity_batched_vs_ref_v42_fp64_per_curve"] = (
         out["engine_parity_batched"] / out["ref_v42_fp64_per_curve"])
+    print(json.dumps(out))
+
+
+def mixed(args):
+    """Uneven batch, fast method (fixed 200 bins): the reference's bls.cu FP64
+    one call per curve on a sample vs the engine batched; light curves/s of the
+    sample are scaled by the sample's share of the batch's fold updates so
+    that both rates refer to the same curve-size distribution."""
+    cs = R.mixed_batch(args.curves, seed=2000)
+    durs = R.C2_DURATIONS
+    rk = RefKernels()
+    rng = np.random.default_rng(0)
+    idx = np.sort(rng.choice(len(cs), size=min(args.sample, len(cs)), replace=False))
+    cost = np.array([len(c[0]) * len(c[3]) for c in cs], np.float64)
+    rk.run_gpu_bls(cs[idx[0]][0], cs[idx[0]][1], cs[idx[0]][3], durs, flux_err=cs[idx[0]][2],
+                   n_bins=200, dtype=np.float64)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in idx:
+        t, y, dy, per = cs[i]
+        rk.run_gpu_bls(t, y, per, durs, flux_err=dy, n_bins=200, dtype=np.float64)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    # seconds per unit of work on the sample, applied to the whole batch
+    ref_rate = len(cs) / (dt * cost.sum() / cost[idx].sum())
+    eng = BLSEngine.get(0)
+    lens = np.array([len(c[0]) for c in cs], np.int64)
+    pt = np.zeros(len(cs) + 1, np.int64)
+    np.cumsum(lens, out=pt[1:])
+    sess = BatchSession(eng, pt, [c[3] for c in cs], list(durs), SearchConfig("fast", n_bins=200),
+                        weighted=True)
+    sess.load(np.concatenate([c[0] for c in cs]), np.concatenate([c[1] for c in cs]),
+              np.concatenate([(1.0 / c[2].astype(np.float64) ** 2).astype(np.float32)
+                              for c in cs]))
+    sess.run()
+    torch.cuda.synchronize()
+    ms = min(sess.plan.profile()["search"] for _ in range(2))
+    out = {"workload": f"uneven batch of {len(cs)} curves (mixed_batch seed 2000), fast method, "
+                       "fixed 200 bins, 8 durations 0.02-0.30 d",
+           "ref_bls_fp64_per_curve": ref_rate, "ref_sample_curves": len(idx),
+           "ref_sample_seconds": dt, "engine_fast_batched": len(cs) / (ms * 1e-3),
+           "engine_ms_search": ms}
+    out["speedup_fast_batched_vs_ref_fp64_per_curve"] = out["engine_fast_batched"] / ref_rate
     print(json.dumps(out))
 
 

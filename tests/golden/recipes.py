@@ -138,3 +138,57 @@ def uniform_batch(n_curves=4096, n=15000, seed=1, transit_fraction=0.3):
         dy[c] = sig
         truth.append(tr)
     return t, y, dy, truth
+
+
+C2_DURATIONS = np.geomspace(0.02, 0.3, 8)
+
+
+def mixed_curve_spec(rng):
+    """One curve of the uneven-batch distribution: N log-uniform in
+    [1e3, 2e5], 1-13 concatenated sectors, 2- or 30-minute cadence (N capped
+    by the cadences available), a frequency-uniform period grid from 0.5 d to
+    baseline/2 with step 1/(84 baseline) in frequency (clipped to 1 000-60 000
+    periods)."""
+    n_sec = int(rng.integers(1, 14))
+    cad = CADENCE_2MIN if rng.uniform() < 0.5 else 30.0 / 1440.0
+    avail = int(n_sec * (SECTOR_DAYS - 1.0) / cad)
+    n = min(int(np.exp(rng.uniform(np.log(1e3), np.log(2e5)))), avail)
+    base = n_sec * SECTOR_DAYS
+    fmin, fmax = 2.0 / base, 2.0
+    n_per = int(np.clip((fmax - fmin) * 84.0 * base, 1000, 60000))
+    return n_sec, cad, n, n_per
+
+
+def mixed_curve(rng, n_sec, cad, n, n_per, t_offset=None, transit_fraction=0.3):
+    """Times (sorted, gaps at each mid-sector), float32 flux with white noise
+    and an optional box transit, float32 dy, and the curve's period grid."""
+    t_offset = rng.uniform(1300.0, 2700.0) if t_offset is None else t_offset
+    grid = []
+    for s in range(n_sec):
+        g = np.arange(0.0, SECTOR_DAYS, cad)
+        lo, hi = 0.5 * (SECTOR_DAYS - 1.0), 0.5 * (SECTOR_DAYS + 1.0)
+        grid.append(t_offset + s * SECTOR_DAYS + g[(g < lo) | (g >= hi)])
+    grid = np.concatenate(grid)
+    t = grid[np.sort(rng.choice(grid.size, size=n, replace=False))]
+    sig = float(np.exp(rng.uniform(np.log(2e-4), np.log(5e-3))))
+    y = 1.0 + rng.normal(0.0, sig, n)
+    if rng.uniform() < transit_fraction:
+        P = rng.uniform(0.5, min(40.0, 0.5 * n_sec * SECTOR_DAYS))
+        y = inject_box(t, y, P, t[0] + rng.uniform(0.0, P), rng.uniform(0.03, 0.25),
+                       rng.uniform(3e-4, 1e-2))
+    base = n_sec * SECTOR_DAYS
+    periods = 1.0 / np.linspace(2.0, 2.0 / base, n_per)
+    return t, y.astype(np.float32), np.full(n, sig, np.float32), periods
+
+
+def mixed_batch(n_curves=8192, seed=2, max_points=None):
+    """Uneven batch: lists of per-curve (t, y, dy, periods); `max_points`
+    optionally caps N (smaller test batches of the same shape family)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n_curves):
+        n_sec, cad, n, n_per = mixed_curve_spec(rng)
+        if max_points is not None:
+            n = min(n, max_points)
+        out.append(mixed_curve(rng, n_sec, cad, n, n_per))
+    return out
