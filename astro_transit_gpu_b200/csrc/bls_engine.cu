@@ -1456,6 +1456,11 @@ struct atb_plan {
     int* best = nullptr;
     int* status = nullptr;
     unsigned long long* counter = nullptr;
+    // plans made by atb_plan_create_async: scratch comes from the stream-ordered
+    // allocator and every set-up copy, the status read-back and the release run
+    // on `stream`, so that no call waits for other streams' work
+    cudaStream_t stream = nullptr;
+    bool async = false;
 };
 
 namespace {
@@ -1484,7 +1489,7 @@ template <typename T>
 int plan_alloc(atb_plan* p, T** out, size_t count) {
     void* ptr = nullptr;
     const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
-    cudaError_t e = cudaMalloc(&ptr, bytes);
+    cudaError_t e = p->async ? cudaMallocAsync(&ptr, bytes, p->stream) : cudaMalloc(&ptr, bytes);
     if (e != cudaSuccess)
         return fail(p->h, ATB_ENOMEM, "cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(e));
     p->allocs.push_back(ptr);
@@ -1497,14 +1502,32 @@ template <typename T>
 int plan_upload(atb_plan* p, T** out, const std::vector<T>& host) {
     int rc = plan_alloc(p, out, host.size());
     if (rc) return rc;
-    if (!host.empty()) ATB_CUDA(p->h, cudaMemcpy(*out, host.data(), host.size() * sizeof(T),
-                                                 cudaMemcpyHostToDevice));
+    if (!host.empty()) {
+        // from pageable memory: returns once the data are staged, so `host` may go
+        ATB_CUDA(p->h, p->async ? cudaMemcpyAsync(*out, host.data(), host.size() * sizeof(T),
+                                                  cudaMemcpyHostToDevice, p->stream)
+                                : cudaMemcpy(*out, host.data(), host.size() * sizeof(T),
+                                             cudaMemcpyHostToDevice));
+    }
     return ATB_OK;
 }
 
 void plan_free(atb_plan* p) {
-    for (void* q : p->allocs) cudaFree(q);
+    for (void* q : p->allocs) {
+        if (p->async)
+            cudaFreeAsync(q, p->stream);
+        else
+            cudaFree(q);
+    }
     p->allocs.clear();
+}
+
+// Device-to-host read of one small value: on the plan's stream for
+// asynchronous plans (waits for that stream only), else synchronous.
+cudaError_t plan_read(atb_plan* p, void* dst, const void* src, size_t bytes) {
+    if (!p->async) return cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost);
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, p->stream);
+    return e == cudaSuccess ? cudaStreamSynchronize(p->stream) : e;
 }
 
 int launch_stage(atb_plan* p, cudaStream_t s) {
@@ -1548,8 +1571,24 @@ int atb_last_error(const atb_handle* h, char* buf, size_t len) {
     return (int)h->err.size();
 }
 
+namespace {
+int plan_create(atb_handle* h, const atb_params* prm, const atb_batch* b, const atb_outputs* o,
+                cudaStream_t stream, bool async, atb_plan** out);
+}  // namespace
+
 int atb_plan_create(atb_handle* h, const atb_params* prm, const atb_batch* b,
                     const atb_outputs* o, atb_plan** out) {
+    return plan_create(h, prm, b, o, nullptr, false, out);
+}
+
+int atb_plan_create_async(atb_handle* h, const atb_params* prm, const atb_batch* b,
+                          const atb_outputs* o, void* stream, atb_plan** out) {
+    return plan_create(h, prm, b, o, static_cast<cudaStream_t>(stream), true, out);
+}
+
+namespace {
+int plan_create(atb_handle* h, const atb_params* prm, const atb_batch* b, const atb_outputs* o,
+                cudaStream_t stream, bool async, atb_plan** out) {
     if (!h) return ATB_EINVAL;
     if (!prm || !b || !o || !out) return fail(h, ATB_EINVAL, "null argument");
     *out = nullptr;
@@ -1618,6 +1657,8 @@ int atb_plan_create(atb_handle* h, const atb_params* prm, const atb_batch* b,
     ATB_CUDA(h, cudaSetDevice(h->device));
     atb_plan* p = new atb_plan();
     p->h = h;
+    p->stream = stream;
+    p->async = async;
     p->prm = *prm;
     p->n_curves = nc;
     p->y_is_f64 = b->y_is_f64 ? 1 : 0;
@@ -1678,10 +1719,11 @@ int atb_plan_create(atb_handle* h, const atb_params* prm, const atb_batch* b,
         // largest bin count over the batch sizes the global-histogram fallback
         int* d_nb = nullptr;
         if ((rc = plan_alloc(p, &d_nb, 1))) { plan_free(p); delete p; return rc; }
-        cudaMemset(d_nb, 0, sizeof(int));
-        nbins_max_kernel<<<nc, 256>>>(nc, d_pbeg, d_pcnt, d_dbeg, d_dcnt, b->periods,
-                                      b->durations, prm->oversample, prm->max_bins, d_nb);
-        cudaError_t e = cudaMemcpy(&nb_max, d_nb, sizeof(int), cudaMemcpyDeviceToHost);
+        cudaMemsetAsync(d_nb, 0, sizeof(int), stream);
+        nbins_max_kernel<<<nc, 256, 0, stream>>>(nc, d_pbeg, d_pcnt, d_dbeg, d_dcnt, b->periods,
+                                                 b->durations, prm->oversample, prm->max_bins,
+                                                 d_nb);
+        cudaError_t e = plan_read(p, &nb_max, d_nb, sizeof(int));
         if (e != cudaSuccess) {
             plan_free(p);
             delete p;
@@ -1771,10 +1813,13 @@ int atb_plan_create(atb_handle* h, const atb_params* prm, const atb_batch* b,
     qa.tile_counter = p->counter;
     qa.status = p->status;
     p->best = o->best_period;
-    ATB_CUDA(h, cudaDeviceSynchronize());
+    // every set-up copy has completed (or, for asynchronous plans, is ordered
+    // before the plan's kernels on its stream)
+    if (!async) ATB_CUDA(h, cudaDeviceSynchronize());
     *out = p;
     return ATB_OK;
 }
+}  // namespace
 
 int atb_plan_execute(atb_plan* p, void* stream) {
     if (!p) return ATB_EINVAL;
@@ -1812,8 +1857,7 @@ int atb_plan_curve_layout(atb_plan* p, int32_t* layout, int32_t* occupancy_bits)
     if (!p || !layout || !occupancy_bits) return ATB_EINVAL;
     ATB_CUDA(p->h, cudaSetDevice(p->h->device));
     std::vector<CurveStat> st(p->n_curves);
-    ATB_CUDA(p->h, cudaMemcpy(st.data(), p->sa.stats, sizeof(CurveStat) * st.size(),
-                              cudaMemcpyDeviceToHost));
+    ATB_CUDA(p->h, plan_read(p, st.data(), p->sa.stats, sizeof(CurveStat) * st.size()));
     for (int c = 0; c < p->n_curves; ++c) {
         layout[c] = st[c].packmode;
         occupancy_bits[c] = st[c].occ_bits;
@@ -1824,7 +1868,7 @@ int atb_plan_curve_layout(atb_plan* p, int32_t* layout, int32_t* occupancy_bits)
 int atb_plan_check(atb_plan* p) {
     if (!p) return ATB_EINVAL;
     int st = 0;
-    ATB_CUDA(p->h, cudaMemcpy(&st, p->status, sizeof(int), cudaMemcpyDeviceToHost));
+    ATB_CUDA(p->h, plan_read(p, &st, p->status, sizeof(int)));
     if (st & 1) return fail(p->h, ATB_EDATA, "input contains non-finite values or weights <= 0");
     if (st & 2) return fail(p->h, ATB_EDATA, "durations must be positive and finite");
     if (st & 4) return fail(p->h, ATB_EDATA, "periods must be positive and finite");

@@ -181,8 +181,11 @@ class SearchPlan:
     """A batch bound to output tensors; ``execute`` enqueues the search."""
 
     def __init__(self, engine: "BLSEngine", batch: CurveBatch, config: SearchConfig,
-                 outputs: Dict[str, torch.Tensor]):
+                 outputs: Dict[str, torch.Tensor], stream: Optional[torch.cuda.Stream] = None):
+        """With `stream`, the plan is set up and released in that stream's
+        order (atb_plan_create_async) and must be executed on it."""
         self.engine = engine
+        self.stream = stream
         self.batch = batch
         self.config = config
         self.outputs = outputs
@@ -213,8 +216,14 @@ class SearchPlan:
         self._params = config.params()
         ptr = ctypes.c_void_p()
         with torch.cuda.device(batch.device):
-            rc = lib.atb_plan_create(engine.handle.ptr, ctypes.byref(self._params),
-                                     ctypes.byref(b), ctypes.byref(o), ctypes.byref(ptr))
+            if stream is None:
+                rc = lib.atb_plan_create(engine.handle.ptr, ctypes.byref(self._params),
+                                         ctypes.byref(b), ctypes.byref(o), ctypes.byref(ptr))
+            else:
+                rc = lib.atb_plan_create_async(engine.handle.ptr, ctypes.byref(self._params),
+                                               ctypes.byref(b), ctypes.byref(o),
+                                               ctypes.c_void_p(stream.cuda_stream),
+                                               ctypes.byref(ptr))
         N.raise_for(rc, engine.handle.ptr, "plan creation")
         self.ptr = ptr
 
@@ -227,7 +236,8 @@ class SearchPlan:
         return int(self._lib.atb_plan_scratch_bytes(self.ptr))
 
     def execute(self, stream: Optional[torch.cuda.Stream] = None) -> None:
-        s = stream if stream is not None else torch.cuda.current_stream(self.batch.device)
+        s = stream if stream is not None else (
+            self.stream or torch.cuda.current_stream(self.batch.device))
         rc = self._lib.atb_plan_execute(self.ptr, ctypes.c_void_p(s.cuda_stream))
         N.raise_for(rc, self.engine.handle.ptr, "plan execution")
 
@@ -320,10 +330,11 @@ class BLSEngine:
         return out
 
     def plan(self, batch: CurveBatch, config: SearchConfig,
-             outputs: Optional[Dict[str, torch.Tensor]] = None) -> SearchPlan:
+             outputs: Optional[Dict[str, torch.Tensor]] = None,
+             stream: Optional[torch.cuda.Stream] = None) -> SearchPlan:
         if outputs is None:
             outputs = self.allocate_outputs(batch)
-        return SearchPlan(self, batch, config, outputs)
+        return SearchPlan(self, batch, config, outputs, stream)
 
     def search(self, batch: CurveBatch, config: SearchConfig,
                stream: Optional[torch.cuda.Stream] = None) -> Dict[str, torch.Tensor]:

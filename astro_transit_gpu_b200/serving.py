@@ -1,0 +1,273 @@
+"""Continuous-batching search server on one GPU.
+
+Requests (one light curve and its own period/duration grid each) are
+submitted from any thread and return a ``concurrent.futures.Future``.  A
+worker thread forms batches from the waiting requests -- first come, first
+served, among requests with the same search configuration -- as long as the
+device-memory budget and the batch size allow, and launches each batch as one
+plan (stage, persistent search, best peak) on one of several CUDA streams.
+Batches already on the GPU keep running while the next ones are formed and
+launched, so requests that arrive meanwhile are admitted as soon as memory
+and a stream are free, and their work overlaps on the device.  A finished
+batch is split into per-request results (the same arrays
+``split_outputs`` gives) and its memory returns to the budget.
+
+Every curve's result depends only on that curve (staging, folding and window
+search are per curve and the arithmetic is exact up to the final FP32/FP64
+formulas), so a request gets the same result alone and in any mix.
+
+Latency is measured per request from ``submit`` to the moment its result is
+ready; :meth:`BLSServer.stats` reports p50/p99 and the completed rate.
+"""
+from __future__ import annotations
+
+import threading
+import time
+from collections import deque
+from concurrent.futures import Future
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional
+
+import numpy as np
+import torch
+
+from .engine import BLSEngine, CurveBatch, SearchConfig, split_outputs
+
+
+@dataclass(eq=False)
+class _Request:
+    t: np.ndarray
+    y: np.ndarray
+    w: Optional[np.ndarray]
+    periods: np.ndarray
+    durations: np.ndarray
+    config: SearchConfig
+    flux_dtype: type
+    nbytes: int
+    arrival: float
+    future: Future = field(default_factory=Future)
+    done: float = 0.0
+
+
+@dataclass(eq=False)
+class _Batch:
+    requests: List[_Request]
+    batch: CurveBatch
+    plan: object
+    stream: torch.cuda.Stream
+    event: torch.cuda.Event
+    nbytes: int
+
+
+def admit(pending, key, held: int, budget: int, max_batch: int):
+    """Form the next batch: the oldest request and the following ones with the
+    same configuration, in arrival order, while the batch has fewer than
+    `max_batch` requests and the bytes held stay within `budget`; the first
+    same-configuration request that does not fit ends the batch (no later one
+    overtakes it).  Returns (batch, remaining requests in order, bytes held)."""
+    pending = deque(pending)
+    if not pending:
+        return [], pending, held
+    k0 = key(pending[0])
+    take, rest, used, closed = [], deque(), held, False
+    for r in pending:
+        if (not closed and key(r) == k0 and len(take) < max_batch
+                and used + r.nbytes <= budget):
+            take.append(r)
+            used += r.nbytes
+        else:
+            if key(r) == k0:
+                closed = True
+            rest.append(r)
+    return take, rest, used
+
+
+def request_bytes(n_points: int, n_periods: int, n_durations: int) -> int:
+    """Device bytes a request holds while its batch runs: inputs (t f64, y, w
+    f32), staged points (16 B), the grids and the per-period outputs (28 B),
+    rounded up for the plan's descriptors."""
+    return int(n_points * (16 + 16) + n_periods * (8 + 28) + n_durations * 8 + 4096)
+
+
+class BLSServer:
+    """Continuous-batching BLS server (one GPU, one worker thread).
+
+    memory_budget  device bytes the in-flight batches may hold (admission)
+    max_batch      most requests in one batch
+    n_streams      batches in flight at once
+    """
+
+    def __init__(self, device=0, memory_budget: float = 120e9, max_batch: int = 512,
+                 n_streams: int = 2):
+        self.engine = BLSEngine.get(device)
+        self.device = self.engine.device
+        self.memory_budget = int(memory_budget)
+        self.max_batch = int(max_batch)
+        self.streams = [torch.cuda.Stream(self.device) for _ in range(max(1, n_streams))]
+        self._pending: deque = deque()
+        self._inflight: List[_Batch] = []
+        self._held = 0
+        self._cv = threading.Condition()
+        self._stop = False
+        self._latencies: List[float] = []
+        self._t_first: Optional[float] = None
+        self._t_last: Optional[float] = None
+        self._batches = 0
+        self._max_held = 0
+        self._worker = threading.Thread(target=self._run, name="bls-server", daemon=True)
+        self._worker.start()
+
+    # ---------------------------------------------------------------- client
+    def submit(self, t, y, dy=None, periods=None, durations=None, method: str = "fast",
+               n_bins: int = 200, objective: Optional[str] = None, oversample: int = 10,
+               max_bins: Optional[int] = None) -> Future:
+        """Queue one search; the future resolves to the curve's per-period
+        outputs (power, depth, depth_err, t0, duration, window) and best_index."""
+        if periods is None or durations is None:
+            raise ValueError("periods and durations must be given")
+        t = np.ascontiguousarray(t, np.float64)
+        y = np.asarray(y)
+        fdt = np.float64 if y.dtype == np.float64 else np.float32
+        y = np.ascontiguousarray(y, fdt)
+        if len(t) != len(y):
+            raise ValueError("time and flux must have the same length")
+        w = None
+        if dy is not None:
+            dy = np.asarray(dy, np.float64)
+            if len(dy) != len(y):
+                raise ValueError("flux_err and flux must have the same length")
+            w = (1.0 / (dy * dy)).astype(np.float32)
+        cfg = (SearchConfig("fast", n_bins=int(n_bins)) if method == "fast" else
+               SearchConfig("parity", objective=objective or "snr", oversample=int(oversample),
+                            max_bins=max_bins))
+        cfg.params()  # validates the combination
+        per = np.atleast_1d(np.asarray(periods, np.float64))
+        dur = np.atleast_1d(np.asarray(durations, np.float64))
+        req = _Request(t, y, w, per, dur, cfg, fdt,
+                       request_bytes(len(t), len(per), len(dur)), time.perf_counter())
+        if req.nbytes > self.memory_budget:
+            raise MemoryError(f"request needs {req.nbytes} bytes, budget {self.memory_budget}")
+        with self._cv:
+            if self._stop:
+                raise RuntimeError("server is closed")
+            self._pending.append(req)
+            self._cv.notify()
+        return req.future
+
+    def stats(self) -> Dict[str, float]:
+        with self._cv:
+            lat = np.array(self._latencies)
+            span = (self._t_last - self._t_first) if self._t_first is not None else 0.0
+            return {
+                "completed": int(lat.size), "batches": self._batches,
+                "p50_ms": float(np.percentile(lat, 50) * 1e3) if lat.size else float("nan"),
+                "p99_ms": float(np.percentile(lat, 99) * 1e3) if lat.size else float("nan"),
+                "mean_ms": float(lat.mean() * 1e3) if lat.size else float("nan"),
+                "curves_per_s": float(lat.size / span) if span > 0 else float("nan"),
+                "max_held_bytes": self._max_held,
+            }
+
+    def close(self) -> None:
+        """Finish every submitted request, then stop the worker."""
+        with self._cv:
+            self._stop = True
+            self._cv.notify()
+        self._worker.join()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---------------------------------------------------------------- worker
+    @staticmethod
+    def _key(r: _Request):
+        c = r.config
+        return (c.method, c.objective, c.n_bins, c.oversample, c.max_bins, r.flux_dtype,
+                r.w is not None)
+
+    def _admit(self) -> List[_Request]:
+        take, self._pending, self._held = admit(self._pending, self._key, self._held,
+                                                self.memory_budget, self.max_batch)
+        self._max_held = max(self._max_held, self._held)
+        return take
+
+    def _launch(self, reqs: List[_Request], stream: torch.cuda.Stream) -> _Batch:
+        with torch.cuda.stream(stream):
+            batch = CurveBatch.from_arrays(
+                [r.t for r in reqs], [r.y for r in reqs],
+                periods=[r.periods for r in reqs], durations=[r.durations for r in reqs],
+                device=self.device, flux_dtype=reqs[0].flux_dtype,
+                weights=[r.w for r in reqs] if reqs[0].w is not None else None)
+            plan = self.engine.plan(batch, reqs[0].config, stream=stream)
+            plan.execute(stream)
+            ev = torch.cuda.Event()
+            ev.record(stream)
+        return _Batch(reqs, batch, plan, stream, ev, sum(r.nbytes for r in reqs))
+
+    def _finish(self, b: _Batch) -> None:
+        try:
+            b.plan.check()
+            outs = split_outputs(b.batch, b.plan.outputs)
+            err = None
+        except Exception as e:  # invalid data: every request of the batch fails
+            outs, err = None, e
+        finally:
+            b.plan.close()
+        now = time.perf_counter()
+        with self._cv:
+            self._held -= b.nbytes
+            self._batches += 1
+            for r in b.requests:
+                r.done = now
+                self._latencies.append(r.done - r.arrival)
+                self._t_first = r.arrival if self._t_first is None else min(self._t_first,
+                                                                            r.arrival)
+                self._t_last = now
+        for i, r in enumerate(b.requests):
+            if err is None:
+                r.future.set_result(outs[i])
+            else:
+                r.future.set_exception(err)
+
+    def _run(self) -> None:
+        try:
+            self._loop()
+        except BaseException as e:  # never leave a client waiting on a dead worker
+            with self._cv:
+                self._stop = True
+                waiting = list(self._pending) + [r for b in self._inflight for r in b.requests]
+                self._pending.clear()
+            for r in waiting:
+                if not r.future.done():
+                    r.future.set_exception(RuntimeError(f"server worker failed: {e!r}"))
+            raise
+
+    def _loop(self) -> None:
+        torch.cuda.set_device(self.device)
+        while True:
+            # retire finished batches
+            for b in [b for b in self._inflight if b.event.query()]:
+                self._inflight.remove(b)
+                self._finish(b)
+            with self._cv:
+                busy = {id(b.stream) for b in self._inflight}
+                free = [s for s in self.streams if id(s) not in busy]
+                reqs = self._admit() if free else []
+                if not reqs:
+                    if self._stop and not self._pending and not self._inflight:
+                        return
+                    if not self._inflight:
+                        self._cv.wait(timeout=0.05)
+                        continue
+            if reqs:
+                try:
+                    self._inflight.append(self._launch(reqs, free[0]))
+                except Exception as e:
+                    with self._cv:
+                        self._held -= sum(r.nbytes for r in reqs)
+                    for r in reqs:
+                        r.future.set_exception(e)
+                continue
+            time.sleep(20e-6)  # batches on the GPU: poll their events

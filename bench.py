@@ -63,6 +63,10 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0,
                     help="target CPU time of the bounded cpu_baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serving-rate", type=float, default=200.0,
+                    help="Poisson arrival rate (requests/s) of the serving measurement")
+    ap.add_argument("--serving-seconds", type=float, default=5.0)
+    ap.add_argument("--no-serving", action="store_true")
     args = ap.parse_args()
     if args.curves is None:
         args.curves = 4096 if args.workload == "uniform" else 8192
@@ -251,6 +255,48 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_serving(args, device):
+    """Continuous-batching server under Poisson arrivals: each request is one
+    curve of the uneven-batch distribution (fast method, 4-8 durations);
+    returns p50/p99 latency from submission to result and the completed rate."""
+    import recipes as R
+    from astro_transit_gpu_b200.serving import BLSServer
+    rng = np.random.default_rng(4000)
+    n_req = max(1, int(args.serving_rate * args.serving_seconds))
+    reqs = []
+    for i in range(n_req):
+        n_sec, cad, n, n_per = R.mixed_curve_spec(rng)
+        t, y, dy, per = R.mixed_curve(rng, n_sec, cad, n, n_per)
+        reqs.append(dict(t=t, y=y, dy=dy, periods=per,
+                         durations=R.C2_DURATIONS[:4 + int(rng.integers(0, 5))], method="fast"))
+    gaps = rng.exponential(1.0 / args.serving_rate, n_req)
+    with BLSServer(device=device, memory_budget=120e9, max_batch=512, n_streams=2) as srv:
+        # warm-up request (library load, allocator pools)
+        srv.submit(**reqs[0]).result(timeout=300)
+        srv._latencies.clear()
+        srv._t_first = srv._t_last = None
+        srv._batches = 0
+        t0 = time.perf_counter()
+        due = t0 + np.cumsum(gaps)
+        futs = []
+        for r, d in zip(reqs, due):
+            wait = d - time.perf_counter()
+            if wait > 0:
+                time.sleep(wait)
+            futs.append(srv.submit(**r))
+        for f in futs:
+            f.result(timeout=300)
+        st = srv.stats()
+    return {"arrivals": "Poisson", "offered_rate_per_s": args.serving_rate,
+            "requests": n_req, "seconds": args.serving_seconds,
+            "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
+            "completed_curves_per_s": st["curves_per_s"], "batches": st["batches"],
+            "request": "one uneven-batch curve (N log-U[1e3, 2e5], 1-13 sectors, 4435-59673 "
+                       "periods), fast method, 4-8 durations 0.02-0.30 d",
+            "admission": "120 GB device-memory budget, up to 512 requests per batch, "
+                         "2 batches in flight"}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -374,6 +420,8 @@ def main():
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
                                 "sample": sample,
                                 "max_rel_power_err_vs_gpu": rel}
+    if world == 1 and not args.no_serving:
+        line["serving"] = run_serving(args, dev)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

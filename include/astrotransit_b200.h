@@ -119,6 +119,16 @@ const char* atb_version(void);
  */
 int atb_plan_create(atb_handle* h, const atb_params* params, const atb_batch* batch,
                     const atb_outputs* outputs, atb_plan** out);
+/*
+ * The same plan, set up without waiting for other streams' work (no reference
+ * counterpart; for servers that overlap batches): its scratch comes from the
+ * stream-ordered allocator on `stream`, its set-up copies and status reads run
+ * on `stream`, and atb_plan_destroy releases it in `stream` order.  The batch's
+ * device inputs must be ready in `stream` order, and the plan must be executed
+ * on `stream`.
+ */
+int atb_plan_create_async(atb_handle* h, const atb_params* params, const atb_batch* batch,
+                          const atb_outputs* outputs, void* stream, atb_plan** out);
 int atb_plan_execute(atb_plan* p, void* stream);
 /* Synchronises `stream`-independent plan state: returns ATB_EDATA if the last
    execution met invalid input data, ATB_OK otherwise. */
