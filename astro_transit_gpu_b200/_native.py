@@ -33,7 +33,7 @@ EXPORTS = (
     "atb_plan_scratch_bytes", "atb_plan_destroy", "atb_search", "atb_run_gpu_bls",
     "atb_run_vbls_exact_parity", "atb_debug_fold", "atb_plan_profile",
     "atb_bench_smem_red_u64", "atb_bench_dfma", "atb_search_curve_static",
-    "atb_plan_curve_layout", "atb_plan_create_async",
+    "atb_plan_curve_layout", "atb_plan_create_async", "atb_plan_top_k",
 )
 
 # limit of atb_search_curve_static (ATB_STATIC_MAX_POINTS in the header)
@@ -98,6 +98,7 @@ def load(build_if_missing: bool = True):
         L.atb_plan_create_async.argtypes = [_vp, ctypes.POINTER(Params), ctypes.POINTER(Batch),
                                             ctypes.POINTER(Outputs), _vp, ctypes.POINTER(_vp)]
         L.atb_plan_execute.argtypes = [_vp, _vp]
+        L.atb_plan_top_k.argtypes = [_vp, _i32, _i32, _vp, _vp]
         L.atb_plan_check.argtypes = [_vp]
         L.atb_plan_kernel_count.argtypes = [_vp]
         L.atb_plan_scratch_bytes.argtypes = [_vp]
@@ -125,7 +126,7 @@ def load(build_if_missing: bool = True):
         for fn in ("atb_search_curve_static", "atb_plan_profile", "atb_bench_smem_red_u64",
                    "atb_bench_dfma",
                    "atb_create", "atb_last_error", "atb_plan_create", "atb_plan_create_async",
-                   "atb_plan_execute",
+                   "atb_plan_execute", "atb_plan_top_k",
                    "atb_plan_check", "atb_plan_kernel_count", "atb_search", "atb_run_gpu_bls",
                    "atb_run_vbls_exact_parity", "atb_debug_fold"):
             getattr(L, fn).restype = ctypes.c_int

@@ -98,16 +98,23 @@ def _config(method: str, n_bins: int, kwargs: Dict[str, Any]) -> SearchConfig:
     raise ValueError(f"unknown method {method!r} (expected 'fast' or 'parity')")
 
 
-def _result(periods, out, cfg: SearchConfig, dtype, n_data: int, orig_periods) -> BLSResult:
+def _result(periods, out, cfg: SearchConfig, dtype, n_data: int, orig_periods,
+            top_idx=None) -> BLSResult:
+    """`top_idx`: the device top-5 peak indices (-1 padded); without them the
+    host find_peaks path of gpu_bls.get_top_k_candidates is used."""
     fdt = np.dtype(dtype)
     fdt = np.float64 if fdt == np.float64 else np.float32
     power = out["power"].astype(fdt, copy=False)
     bi = int(out["best_index"]) if out.get("best_index", -1) >= 0 else int(np.argmax(power))
-    raw = {"power": power, "all_t0s": out["t0"], "all_durs": out["duration"],
-           "all_depths": out["depth"], "periods": periods}
-    top = [Candidate(float(c["period"]), float(c["t0"]), float(c["duration"]),
-                     float(c["depth"]), float(c["power"]))
-           for c in get_top_k_candidates(raw, k=5)]
+    if top_idx is not None:
+        top = [Candidate(float(periods[i]), float(out["t0"][i]), float(out["duration"][i]),
+                         float(out["depth"][i]), float(power[i])) for i in top_idx if i >= 0]
+    else:
+        raw = {"power": power, "all_t0s": out["t0"], "all_durs": out["duration"],
+               "all_depths": out["depth"], "periods": periods}
+        top = [Candidate(float(c["period"]), float(c["t0"]), float(c["duration"]),
+                         float(c["depth"]), float(c["power"]))
+               for c in get_top_k_candidates(raw, k=5)]
     meta = {"n_bins": cfg.n_bins if cfg.method == "fast" else cfg.max_bins,
             "dtype": str(dtype), "n_data": n_data, "method": cfg.method,
             "objective": cfg.objective or ("fast" if cfg.method == "fast" else "snr"),
@@ -176,5 +183,13 @@ def power_batch(times: Sequence[np.ndarray], fluxes: Sequence[np.ndarray],
                                    periods=checked_p if per_curve_p else checked_p[0],
                                    durations=checked_d if per_curve_d else checked_d[0],
                                    flux_dtype=fdt)
-    outs = split_outputs(batch, BLSEngine.get().search(batch, cfg))
-    return [_result(p, o, cfg, dtype, len(y), p) for p, o, y in zip(checked_p, outs, fluxes)]
+    plan = BLSEngine.get().plan(batch, cfg)
+    try:
+        plan.execute()
+        plan.check()
+        top = plan.top_k(5, 10).cpu().numpy()  # peaks found on the device
+        outs = split_outputs(batch, plan.outputs)
+    finally:
+        plan.close()
+    return [_result(p, o, cfg, dtype, len(y), p, top_idx=tk)
+            for p, o, y, tk in zip(checked_p, outs, fluxes, top)]

@@ -1329,6 +1329,99 @@ __global__ void best_kernel(int n_curves, const long long* per_cnt, const long l
     if (lane == 0) best[warp] = cnt > 0 ? (int)bi : -1;
 }
 
+// ----------------------------------------------------------------------------
+// top-k peaks of each curve's power spectrum (replaces the host
+// scipy.signal.find_peaks(power, distance) + sort of gpu_bls.py:146-174)
+// ----------------------------------------------------------------------------
+
+constexpr int kTopKMax = 32;
+constexpr int kTopKBlock = 256;
+
+// Block-wide argmax of (value, index): larger value, then higher index (the
+// order of a stable ascending sort read from the end, as the reference's
+// argsort(...)[::-1]); index -1 marks "none".
+__device__ void block_argmax(float& v, long long& i, float* sv, long long* si) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const float ov = __shfl_xor_sync(0xffffffffu, v, off);
+        const long long oi = __shfl_xor_sync(0xffffffffu, i, off);
+        if (ov > v || (ov == v && oi > i)) { v = ov; i = oi; }
+    }
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) { sv[w] = v; si[w] = i; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k < kTopKBlock / 32; ++k)
+            if (sv[k] > v || (sv[k] == v && si[k] > i)) { v = sv[k]; i = si[k]; }
+        sv[0] = v;
+        si[0] = i;
+    }
+    __syncthreads();
+    v = sv[0];
+    i = si[0];
+    __syncthreads();
+}
+
+// One CTA per curve.  A peak is the midpoint (l + r) / 2 of a maximal run
+// x[l..r] of equal values with x[l-1] < x[l] and x[r+1] < x[r], 1 <= l,
+// r <= n-2 (scipy's _local_maxima_1d); only the run's first index scans it,
+// so a round costs O(n).  Rounds pick the largest peak at least `distance`
+// samples away from every peak already picked -- the order in which scipy's
+// distance filter keeps peaks -- so the first k picks are scipy's top k.
+// Without any peak, the k largest values are returned (the reference's
+// fallback).  Equal values go to the higher index.
+__global__ void __launch_bounds__(kTopKBlock) topk_peaks_kernel(
+    int n_curves, const long long* per_cnt, const long long* out_beg, const float* power, int k,
+    int distance, int* out_idx) {
+    __shared__ float sv[kTopKBlock / 32];
+    __shared__ long long si[kTopKBlock / 32];
+    __shared__ long long kept[kTopKMax];
+    const int c = blockIdx.x;
+    if (c >= n_curves) return;
+    const long long n = per_cnt[c];
+    const float* x = power + out_beg[c];
+    int nk = 0;
+    bool fallback = false;
+    for (int round = 0; round < k; ++round) {
+        float bv = -INFINITY;
+        long long bi = -1;
+        for (long long l = threadIdx.x; l < n; l += kTopKBlock) {
+            long long m = l;
+            const float v = x[l];
+            if (!fallback) {
+                if (l < 1 || l > n - 2 || !(x[l - 1] < v)) continue;
+                long long r = l;
+                while (r < n - 1 && x[r + 1] == v) ++r;
+                if (r > n - 2 || !(x[r + 1] < v)) continue;
+                m = (l + r) / 2;
+            }
+            bool alive = true;
+            for (int q = 0; q < nk; ++q) {
+                const long long dd = m > kept[q] ? m - kept[q] : kept[q] - m;
+                if (fallback ? dd == 0 : dd < distance) alive = false;
+            }
+            if (alive && (v > bv || (v == bv && m > bi))) {
+                bv = v;
+                bi = m;
+            }
+        }
+        block_argmax(bv, bi, sv, si);
+        if (bi < 0) {
+            if (round == 0 && !fallback && n > 0) {  // no peak at all
+                fallback = true;
+                --round;
+                continue;
+            }
+            break;
+        }
+        if (threadIdx.x == 0) kept[nk] = bi;
+        __syncthreads();
+        ++nk;
+    }
+    for (int q = threadIdx.x; q < k; q += kTopKBlock)
+        out_idx[(long long)c * k + q] = q < nk ? (int)kept[q] : -1;
+}
+
 // per-point histogram slots of curve 0 for every period (verification only):
 // the same staged points, chunking and fold_slots code as the search kernel
 template <int GEOM>
@@ -2029,6 +2122,18 @@ int atb_debug_fold(atb_handle* h, const atb_params* prm, const double* t, const 
     return rc;
 }
 
+
+int atb_plan_top_k(atb_plan* p, int32_t k, int32_t distance, int32_t* out_idx, void* stream) {
+    if (!p || !out_idx) return ATB_EINVAL;
+    if (k < 1 || k > kTopKMax) return fail(p->h, ATB_EINVAL, "k=%d outside [1, %d]", k, kTopKMax);
+    if (distance < 1) return fail(p->h, ATB_EINVAL, "distance=%d must be >= 1", distance);
+    if (!p->qa.power) return fail(p->h, ATB_EINVAL, "the plan has no per-period power output");
+    ATB_CUDA(p->h, cudaSetDevice(p->h->device));
+    topk_peaks_kernel<<<p->n_curves, kTopKBlock, 0, static_cast<cudaStream_t>(stream)>>>(
+        p->n_curves, p->qa.per_cnt, p->qa.out_beg, p->qa.power, k, distance, out_idx);
+    ATB_CUDA(p->h, cudaGetLastError());
+    return ATB_OK;
+}
 
 int atb_plan_profile(atb_plan* p, void* stream, float* ms_stage, float* ms_search,
                      float* ms_best) {

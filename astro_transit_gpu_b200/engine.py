@@ -251,6 +251,19 @@ class SearchPlan:
         N.raise_for(rc, self.engine.handle.ptr, "plan profile")
         return {"stage": ms[0].value, "search": ms[1].value, "best": ms[2].value}
 
+    def top_k(self, k: int = 5, distance: int = 10,
+              stream: Optional[torch.cuda.Stream] = None) -> torch.Tensor:
+        """Device top-k peaks of every curve's power after an execution:
+        int32 [n_curves, k] period indices (largest peak first, -1 padding),
+        as the reference's find_peaks(power, distance) + sort."""
+        s = stream if stream is not None else (
+            self.stream or torch.cuda.current_stream(self.batch.device))
+        out = torch.empty((self.batch.n_curves, k), dtype=torch.int32, device=self.batch.device)
+        rc = self._lib.atb_plan_top_k(self.ptr, int(k), int(distance), _ptr(out),
+                                      ctypes.c_void_p(s.cuda_stream))
+        N.raise_for(rc, self.engine.handle.ptr, "top-k peaks")
+        return out
+
     def curve_layout(self):
         """After an execution: (layout, occupancy_bits) per curve, numpy int32.
         layout is ATB_LAYOUT_SPLIT / COUNT / TIGHT (0 / 1 / 2), the histogram

@@ -44,11 +44,44 @@ def run_gpu_bls(time, flux, periods, durations, flux_err=None, n_bins=200, dtype
     }
 
 
+def top_peak_indices(power, k=5, distance=10):
+    """Indices of the k largest peaks of `power` at least `distance` samples
+    apart, largest first: the local maxima of scipy.signal.find_peaks (flat
+    tops reported at their midpoint), the distance rule of find_peaks(distance)
+    -- peaks taken by decreasing power, each removing the others closer than
+    `distance` -- and, without any peak, the k largest values
+    (gpu_bls.py:156-163).  Equal powers are taken higher index first in every
+    step (a stable sort read from the end); scipy leaves that order to its
+    unstable default sort, so only exact ties can differ from it."""
+    from scipy.signal import find_peaks
+    power = np.asarray(power)
+    peaks, _ = find_peaks(power)
+    if len(peaks) == 0:
+        return [int(i) for i in np.argsort(power, kind="stable")[-k:][::-1]]
+    order = np.argsort(power[peaks], kind="stable")
+    keep = np.ones(len(peaks), bool)
+    picked = []
+    for j in order[::-1]:
+        if not keep[j]:
+            continue
+        picked.append(int(peaks[j]))
+        if len(picked) == k:
+            break
+        lo = j - 1
+        while lo >= 0 and peaks[j] - peaks[lo] < distance:
+            keep[lo] = False
+            lo -= 1
+        hi = j + 1
+        while hi < len(peaks) and peaks[hi] - peaks[j] < distance:
+            keep[hi] = False
+            hi += 1
+    return picked
+
+
 def get_top_k_candidates(results, k=5, min_dist_bins=10):
     """Top-k local maxima of the power spectrum (gpu_bls.py:146-174): peaks of
-    ``scipy.signal.find_peaks(power, distance=min_dist_bins)`` ordered by
-    power, or the k largest powers when there is no peak."""
-    from scipy.signal import find_peaks
+    ``find_peaks(power, distance=min_dist_bins)`` ordered by power, or the k
+    largest powers when there is no peak (see ``top_peak_indices``)."""
 
     def host(a):
         return a.get() if hasattr(a, "get") else np.asarray(a)
@@ -58,10 +91,6 @@ def get_top_k_candidates(results, k=5, min_dist_bins=10):
     durs = host(results["all_durs"])
     depths = host(results["all_depths"])
     periods = results["periods"]
-    peaks, _ = find_peaks(power, distance=min_dist_bins)
-    if len(peaks) == 0:
-        peaks = np.argsort(power)[-k:][::-1]
-    order = np.argsort(power[peaks])[::-1]
-    top = peaks[order[:k]]
+    top = top_peak_indices(power, k, min_dist_bins)
     return [{"period": float(periods[i]), "t0": float(t0s[i]), "duration": float(durs[i]),
              "depth": float(depths[i]), "power": float(power[i])} for i in top]

@@ -140,6 +140,17 @@ int64_t atb_plan_scratch_bytes(const atb_plan* p);
 void atb_plan_destroy(atb_plan* p);
 
 /*
+ * Top-k peaks of each curve's power spectrum after an execution, on the device
+ * (replaces the host scipy.signal.find_peaks(power, distance) + sort of
+ * search/gpu_bls.py:146-174 for batches): out_idx [n_curves * k] int32 receives
+ * per curve the period indices of the k largest peaks at least `distance`
+ * samples apart, largest first (equal powers: higher index first), -1 where
+ * there are fewer; with no peak at all, the k largest powers.  1 <= k <= 32.
+ * Enqueued on `stream`.
+ */
+int atb_plan_top_k(atb_plan* p, int32_t k, int32_t distance, int32_t* out_idx, void* stream);
+
+/*
  * Diagnostics (no reference counterpart): after an atb_plan_execute has
  * completed, the histogram word layout each curve used and the bit length of
  * its bin-occupancy bound (64: no bound).  Layouts: ATB_LAYOUT_SPLIT (weights

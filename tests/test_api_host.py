@@ -78,3 +78,22 @@ def test_no_cpu_fallback_without_cuda():
         BoxLeastSquaresGPU(t, y, dy).power([1.0, 2.0], [0.1], method="parity")
     with pytest.raises((RuntimeError, AssertionError)):
         CurveBatch.from_arrays([t], [y], periods=[1.0], durations=[0.1])
+
+
+def test_top_peak_indices_matches_find_peaks_without_ties():
+    """On spectra without exact ties the host top-k equals scipy's
+    find_peaks(distance) followed by the reference's sort."""
+    from scipy.signal import find_peaks
+    from astro_transit_gpu_b200.gpu_bls import top_peak_indices
+    rng = np.random.default_rng(5)
+    for n, k, dist in ((500, 5, 10), (2000, 8, 3), (50, 5, 1), (3, 5, 10)):
+        x = rng.permutation(n).astype(np.float64) + rng.uniform(0, 0.5, n)
+        x = np.convolve(x, np.ones(3) / 3, mode="same")
+        peaks, _ = find_peaks(x, distance=dist)
+        if len(peaks) == 0:
+            ref = list(np.argsort(x)[-k:][::-1])
+        else:
+            ref = list(peaks[np.argsort(x[peaks])[::-1][:k]])
+        assert top_peak_indices(x, k, dist) == [int(i) for i in ref]
+    # equal powers: the higher index first
+    assert top_peak_indices(np.array([0, 2, 0, 2, 0.0]), 2, 1) == [3, 1]
