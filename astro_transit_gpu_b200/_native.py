@@ -61,7 +61,7 @@ class Batch(ctypes.Structure):
 
 class Outputs(ctypes.Structure):
     _fields_ = [("power", _vp), ("depth", _vp), ("depth_err", _vp), ("t0", _vp),
-                ("duration", _vp), ("window", _vp), ("best_period", _vp)]
+                ("duration", _vp), ("window", _vp), ("best_period", _vp), ("best_key", _vp)]
 
 
 class NativeError(RuntimeError):

@@ -180,6 +180,7 @@ struct SearchArgs {
     long long ghist_stride;
     unsigned long long* tile_counter;
     int* status;
+    unsigned long long* best_key;  // winner-take-all per-curve records (or NULL)
 };
 
 // ----------------------------------------------------------------------------
@@ -1174,7 +1175,15 @@ __device__ void finalize_period(const SearchArgs& a, GroupSmem& gs, const Team& 
             o_de = (float)de;
             o_win = best.key;
         }
-        a.power[slot] = o_pw;
+        if (a.best_key && o_win >= 0) {
+            // (power bits << 32 | ~period index): non-negative floats order
+            // like their bits, and among equal powers the lowest index wins
+            const unsigned long long key =
+                ((unsigned long long)__float_as_uint(o_pw) << 32) |
+                (unsigned long long)(0xffffffffu - (unsigned)(slot - a.out_beg[gs.curve]));
+            atomicMax(a.best_key + gs.curve, key);
+        }
+        if (a.power) a.power[slot] = o_pw;
         if (a.depth) a.depth[slot] = o_dep;
         if (a.depth_err) a.depth_err[slot] = o_de;
         if (a.t0) a.t0[slot] = o_t0;
@@ -1308,10 +1317,17 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) search_kernel(const Search
 
 // per-curve argmax over the grid (first maximum, as cupy.argmax)
 __global__ void best_kernel(int n_curves, const long long* per_cnt, const long long* out_beg,
-                            const float* power, int* best) {
+                            const float* power, const unsigned long long* best_key, int* best) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= n_curves) return;
+    if (!power) {  // winner-take-all: the packed record holds the index
+        if (lane == 0) {
+            const unsigned long long k = best_key[warp];
+            best[warp] = k ? (int)(0xffffffffu - (unsigned)(k & 0xffffffffu)) : -1;
+        }
+        return;
+    }
     const long long cnt = per_cnt[warp];
     const float* pw = power + out_beg[warp];
     float bv = -INFINITY;
@@ -1708,7 +1724,8 @@ int plan_create(atb_handle* h, const atb_params* prm, const atb_batch* b, const 
         return fail(h, ATB_EINVAL, "batch index arrays must not be NULL");
     if (!b->t || !b->y || !b->periods || !b->durations)
         return fail(h, ATB_EINVAL, "batch data pointers must not be NULL");
-    if (!o->power) return fail(h, ATB_EINVAL, "outputs.power must not be NULL");
+    if (!o->power && !o->best_key)
+        return fail(h, ATB_EINVAL, "outputs.power and outputs.best_key must not both be NULL");
 
     std::vector<long long> pt_off(nc + 1), t_off(nc), per_beg(nc), per_cnt(nc), dur_beg(nc),
         out_beg(nc), stage_off(nc), tile_off(nc + 1);
@@ -1896,6 +1913,7 @@ int plan_create(atb_handle* h, const atb_params* prm, const atb_batch* b, const 
     qa.stats = d_stats;
     qa.dbins = d_dbins;
     qa.power = o->power;
+    qa.best_key = reinterpret_cast<unsigned long long*>(o->best_key);
     qa.depth = o->depth;
     qa.depth_err = o->depth_err;
     qa.t0 = o->t0;
@@ -1933,7 +1951,7 @@ int atb_plan_execute(atb_plan* p, void* stream) {
         const int threads = 256;
         const int blocks = (p->n_curves * 32 + threads - 1) / threads;
         best_kernel<<<blocks, threads, 0, s>>>(p->n_curves, p->qa.per_cnt, p->qa.out_beg,
-                                               p->qa.power, p->best);
+                                               p->qa.power, p->qa.best_key, p->best);
         ATB_CUDA(h, cudaGetLastError());
     }
     return ATB_OK;
@@ -2159,7 +2177,7 @@ int atb_plan_profile(atb_plan* p, void* stream, float* ms_stage, float* ms_searc
     if (!rc && p->best) {
         const int blocks = (p->n_curves * 32 + 255) / 256;
         best_kernel<<<blocks, 256, 0, s>>>(p->n_curves, p->qa.per_cnt, p->qa.out_beg,
-                                           p->qa.power, p->best);
+                                           p->qa.power, p->qa.best_key, p->best);
     }
     ATB_CUDA(h, cudaEventRecord(ev[3], s));
     ATB_CUDA(h, cudaEventSynchronize(ev[3]));
@@ -2474,7 +2492,8 @@ extern "C" int atb_search_curve_static(const atb_params* prm, const double* t, c
         search_kernel<ATB_GEOM_BINNED><<<grid, kBlock, dyn, s>>>(qa);
     else
         search_kernel<ATB_GEOM_FIXED><<<grid, kBlock, dyn, s>>>(qa);
-    if (best_index) best_kernel<<<1, 32, 0, s>>>(1, m->per_cnt, m->out_beg, power, best_index);
+    if (best_index)
+        best_kernel<<<1, 32, 0, s>>>(1, m->per_cnt, m->out_beg, power, nullptr, best_index);
     e = cudaGetLastError();
     if (e != cudaSuccess)
         return static_fail(err, err_len, ATB_ECUDA, "launch: %s", cudaGetErrorString(e));

@@ -213,6 +213,7 @@ class SearchPlan:
         for k in OUTPUT_FIELDS:
             setattr(o, k, _ptr(outputs.get(k)))
         o.best_period = _ptr(outputs.get("best_period"))
+        o.best_key = _ptr(outputs.get("best_key"))
         self._params = config.params()
         ptr = ctypes.c_void_p()
         with torch.cuda.device(batch.device):
@@ -348,6 +349,43 @@ class BLSEngine:
         if outputs is None:
             outputs = self.allocate_outputs(batch)
         return SearchPlan(self, batch, config, outputs, stream)
+
+    def screen(self, batch: CurveBatch, config: SearchConfig,
+               stream: Optional[torch.cuda.Stream] = None) -> Dict[str, torch.Tensor]:
+        """Winner-take-all search (the reference's screening mode keeps only a
+        best record per target): no per-period array is written -- each
+        period raises its curve's packed (power, ~index) record with an
+        atomicMax -- then every curve's winning period is searched once more
+        to report its window.  Returns per-curve tensors best_index (int32, -1
+        when no period has a valid window), period, power, depth, depth_err,
+        t0, duration, window: what the full search reports at its best period
+        (synchronises)."""
+        s = stream if stream is not None else torch.cuda.current_stream(batch.device)
+        nc = batch.n_curves
+        with torch.cuda.stream(s):
+            key = torch.zeros(nc, dtype=torch.int64, device=batch.device)
+            best = torch.empty(nc, dtype=torch.int32, device=batch.device)
+        plan = self.plan(batch, config, {"best_key": key, "best_period": best})
+        try:
+            plan.execute(s)
+            plan.check()
+        finally:
+            plan.close()
+        # the winning period of every curve, gathered on the device
+        with torch.cuda.stream(s):
+            pbeg = torch.from_numpy(_i64(batch.period_begin)).to(batch.device)
+            idx = torch.clamp(best.to(torch.int64), min=0) + pbeg
+            win_p = batch.periods[idx].contiguous()
+        one = CurveBatch(t=batch.t, y=batch.y, w=batch.w, periods=win_p,
+                         durations=batch.durations, point_offset=batch.point_offset,
+                         period_begin=np.arange(nc, dtype=np.int64),
+                         period_count=np.ones(nc, np.int64), dur_begin=batch.dur_begin,
+                         dur_count=batch.dur_count, out_begin=np.arange(nc, dtype=np.int64),
+                         time_offset=batch.time_offset)
+        out = {k: v for k, v in self.search(one, config, s).items() if k != "best_period"}
+        out["best_index"] = best
+        out["period"] = win_p
+        return out
 
     def search(self, batch: CurveBatch, config: SearchConfig,
                stream: Optional[torch.cuda.Stream] = None) -> Dict[str, torch.Tensor]:

@@ -99,6 +99,13 @@ typedef struct {
     float* duration;       /* BINNED: dur_bins*bin_duration; FIXED: the duration grid value */
     int32_t* window;       /* start_bin * n_durations + duration_index, -1 when no valid window */
     int32_t* best_period;  /* [n_curves]: index of the maximum power within the curve's grid */
+    /* Winner-take-all screening (search/vbls.py:62-188 keeps only a best record
+     * per target): [n_curves] packed (power bits << 32 | ~period index),
+     * raised with atomicMax, zeroed by the caller before the execution.  With
+     * it, every per-period array above may be NULL (nothing per period is
+     * written) and best_period is decoded from it (first maximum; -1 when no
+     * period has a valid window). */
+    uint64_t* best_key;
 } atb_outputs;
 
 /* Handle: one per device (and per host thread using it concurrently). */

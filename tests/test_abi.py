@@ -46,4 +46,4 @@ def test_structs_match_header_layout():
     # int32 x6 params; batch: 2 ints + 7 host pointers + 5 device pointers
     assert ctypes.sizeof(N.Params) == 24
     assert ctypes.sizeof(N.Batch) == 8 + 12 * 8
-    assert ctypes.sizeof(N.Outputs) == 7 * 8
+    assert ctypes.sizeof(N.Outputs) == 8 * 8

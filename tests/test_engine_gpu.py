@@ -347,3 +347,32 @@ def test_batch_session_graph_replay_matches_eager(engine):
     torch.cuda.synchronize()
     for k in ref:
         assert torch.equal(graphed.host_out[k], eager.host_out[k]), k
+
+
+# ------------------------------------------------------ winner-take-all ---
+
+@pytest.mark.parametrize("method", ["fast", "parity"])
+def test_screen_equals_full_search_at_its_best_period(engine, method):
+    """The winner-take-all mode (no per-period output, packed atomicMax per
+    curve, then the winner searched again) reports exactly what the full
+    search reports at its best period."""
+    from astro_transit_gpu_b200.engine import CurveBatch, SearchConfig
+    rng = np.random.default_rng(31)
+    ts, ys, es, ps = [], [], [], []
+    for i in range(7):
+        n_sec, cad, n, n_per = R.mixed_curve_spec(rng)
+        t, y, dy, per = R.mixed_curve(rng, n_sec, cad, min(n, 8000), min(n_per, 3000))
+        ts.append(t); ys.append(1.0 + y); es.append(dy); ps.append(per)
+    cfg = (SearchConfig("fast", n_bins=128) if method == "fast" else
+           SearchConfig("parity", objective="likelihood"))
+    b = CurveBatch.from_arrays(ts, ys, es, periods=ps, durations=R.C2_DURATIONS[:6],
+                               device=engine.device)
+    full = {k: v.cpu().numpy() for k, v in engine.search(b, cfg).items()}
+    scr = {k: v.cpu().numpy() for k, v in engine.screen(b, cfg).items()}
+    for c in range(b.n_curves):
+        bi = int(full["best_period"][c])
+        assert int(scr["best_index"][c]) == bi
+        g = int(b.out_begin[c]) + bi
+        assert scr["period"][c] == ps[c][bi]
+        for k in FIELDS:
+            assert scr[k][c] == full[k][g], (c, k)
