@@ -9,6 +9,9 @@ kernels see exactly the arguments the reference passes:
 
 * ``run_gpu_bls``            search/gpu_bls.py:42-144
 * ``run_vbls_exact_parity``  search/v42_parity.py:27-107
+* ``run_vbls_massive``       search/vbls.py:62-188 (the batched screening
+                             kernel, built for 1312 points, 128 bins, 8
+                             durations, float)
 
 Device memory is managed with PyTorch, kernels are loaded and launched with
 the CUDA driver API (cuda-python).  The elementwise prologue and the totals
@@ -56,6 +59,12 @@ class RefKernels:
             mod = _check(cu.cuModuleLoadData(data))
             self.mods[name] = mod
             self.funcs[name] = _check(cu.cuModuleGetFunction(mod, fn.encode()))
+        v39 = os.path.join(REF_DIR, "v39_f32_n1312_b128_d8.cubin")
+        if os.path.exists(v39):
+            with open(v39, "rb") as f:
+                mod = _check(cu.cuModuleLoadData(f.read()))
+            self.mods["v39"] = mod
+            self.funcs["v39"] = _check(cu.cuModuleGetFunction(mod, b"vbls_v39_weighted_kernel"))
         dev = _check(cu.cuCtxGetDevice())
         self.max_shm = _check(cu.cuDeviceGetAttribute(
             cu.CUdevice_attribute.CU_DEVICE_ATTRIBUTE_MAX_SHARED_MEMORY_PER_BLOCK, dev))
@@ -165,3 +174,48 @@ class RefKernels:
         power, t0, dur, dep = (o.reshape(n_targets, n_periods).cpu().numpy() for o in outs)
         return {"power": power, "t0": t0, "duration": dur, "depth": dep,
                 "best_index": np.argmax(power, axis=1)}
+
+    def run_vbls_massive(self, time_array, flux_matrix, periods, durations, weights_matrix=None,
+                         target_batch_size=4000, period_batch_size=20000, sync=True):
+        """search/vbls.py:62-188 with the Blackwell kernel (float, 128 bins,
+        1312 points, 8 durations): per-target best power (SNR), t0, duration,
+        depth and period, as torch tensors on the device."""
+        if "v39" not in self.funcs:
+            raise FileNotFoundError("oracle/_ref/v39_f32_n1312_b128_d8.cubin missing")
+        dev = self.device
+
+        def on_dev(x):
+            x = x if isinstance(x, torch.Tensor) else torch.as_tensor(np.asarray(x))
+            return x.to(dev).to(torch.float32).contiguous()
+
+        fm = on_dev(flux_matrix)
+        n_t, n_data = fm.shape
+        if n_data != 1312 or len(durations) != 8:
+            raise ValueError("the compiled screening kernel takes 1312 points and 8 durations")
+        tg = torch.as_tensor(np.asarray(time_array), device=dev).to(torch.float32)
+        t_start = float(tg[0].item())
+        dt = (tg - t_start).to(torch.float32).contiguous()
+        wm = torch.ones_like(fm) if weights_matrix is None else on_dev(weights_matrix)
+        durs = np.asarray(durations, np.float32)
+        res = cu.cuModuleGetGlobal(self.mods["v39"], b"c_durations")
+        _check(res[0])
+        _check(cu.cuMemcpyHtoD(res[1], durs.ctypes.data, durs.nbytes))
+        outs = [torch.zeros(n_t, dtype=torch.float32, device=dev) for _ in range(5)]
+        per = np.asarray(periods, np.float32)
+        smem = 3 * n_data * 4 + 2 * 16 * (128 + 1) * 4
+        for p0 in range(0, len(per), period_batch_size):
+            pb = per[p0:p0 + period_batch_size]
+            pairs = torch.as_tensor(np.stack([pb, (1.0 / pb).astype(np.float32)], 1),
+                                    device=dev).contiguous()
+            for t0 in range(0, n_t, target_batch_size):
+                t1 = min(t0 + target_batch_size, n_t)
+                self._launch("v39", ((len(pb) + 15) // 16, t1 - t0), 512, smem, [
+                    ("p", fm[t0].data_ptr()), ("p", dt.data_ptr()), ("p", pairs.data_ptr()),
+                    ("p", wm[t0].data_ptr())] +
+                    [("p", o[t0].data_ptr()) for o in (outs[0], outs[1], outs[2], outs[3],
+                                                       outs[4])] +
+                    [("i", len(pb)), ("f", t_start)])
+        if sync:
+            torch.cuda.synchronize(dev)
+        return {"snr": outs[0], "best_t0": outs[1], "best_duration": outs[2],
+                "best_depth": outs[3], "best_period": outs[4]}
