@@ -570,9 +570,16 @@ struct GroupSmem {
     int curve;
     int G;
     int total;
-    int glob;
+    int glob;        // 0 shared-memory group, 1 global histogram, 2 bin-range passes
     int safe_floor;  // |dt / P| < 2^50 over the group: floor via floor_magic
+    // bin-range passes (one period whose bins exceed shared memory)
+    uint4 pad_save[16];  // raw entries of bins 1..oversample (the V42 padding source)
+    longlong2 carry;     // exact sums of every bin below the next pass
+    longlong2 mp_e0, mp_e1;  // prefix entries of the best window so far
+    float mp_num, mp_den;
+    int mp_key;
 };
+constexpr int kMpPadMax = 16;  // oversample limit of the bin-range passes
 
 // Histogram slots of one thread's kR points for one period, returned as
 // t = slot - 1.
@@ -653,9 +660,11 @@ __device__ __forceinline__ void hist_add_point(unsigned base1, uint4* H1, int t,
 // Fold every staged point of the curve into the group's histograms: one
 // reduction per histogram word and point (merging runs of equal bins costs
 // more issue slots than the reductions it saves).
-template <int GEOM, bool GLOB, int MODE>
+// WIN: bin-range pass -- only slots lo .. lo+W-1 are kept, at entries
+// 0 .. W-1 of H (one period at offset 0).
+template <int GEOM, bool GLOB, int MODE, bool WIN = false>
 __device__ void fold_group(const SearchArgs& a, const GroupSmem& gs, uint4* H, long long so,
-                           long long n_pad, const CurveStat& st) {
+                           long long n_pad, const CurveStat& st, int lo = 0, unsigned W = 0) {
     const int G = gs.G;
     const bool safe = gs.safe_floor != 0;
     const int L = st.lobits;
@@ -708,8 +717,15 @@ __device__ void fold_group(const SearchArgs& a, const GroupSmem& gs, uint4* H, l
             uint4* H1 = H + nbb.y + 1;
             const unsigned base1 = GLOB ? 0u : (unsigned)__cvta_generic_to_shared(H1);
 #pragma unroll
-            for (int j = 0; j < kR; ++j)
-                hist_add_point<GLOB, MODE>(base1, H1, t[j], wa[j], wb[j], wc[j], wd[j]);
+            for (int j = 0; j < kR; ++j) {
+                if (WIN) {
+                    const int tt = t[j] - lo;  // entry tt + 1 of the pass
+                    if ((unsigned)(tt + 1) < W)
+                        hist_add_point<GLOB, MODE>(base1, H1, tt, wa[j], wb[j], wc[j], wd[j]);
+                } else {
+                    hist_add_point<GLOB, MODE>(base1, H1, t[j], wa[j], wb[j], wc[j], wd[j]);
+                }
+            }
         }
     }
 }
@@ -761,7 +777,11 @@ __device__ __forceinline__ void entry_sums(const uint4* R, int i, const CurveSta
     if (st.packmode != kPackSplit && !st.cnt_win) w *= (long long)st.qw0;
 }
 
-__device__ void team_scan(const Team& tm, GroupSmem& gs, longlong2* E, int M, const CurveStat& st) {
+// cw0, cy0: exact sums added to every prefix (the bins below E[0]); the
+// thread holding entry carry_idx stores that entry's exact prefix in *carry.
+__device__ void team_scan(const Team& tm, GroupSmem& gs, longlong2* E, int M, const CurveStat& st,
+                          long long cw0 = 0, long long cy0 = 0, int carry_idx = -1,
+                          longlong2* carry = nullptr) {
     int seg = (M + tm.nthreads - 1) / tm.nthreads;
     seg |= 1;
     const int b = min(M, tm.tid * seg);
@@ -799,8 +819,16 @@ __device__ void team_scan(const Team& tm, GroupSmem& gs, longlong2* E, int M, co
         iw += ow;
         iy += oy;
     }
-    long long xw = iw - sw, xy = iy - sy;
+    long long xw = iw - sw + cw0, xy = iy - sy + cy0;
     const double sy2 = ldexp(1.0, -st.ey);
+    if (carry_idx >= b && carry_idx < e) {
+        long long cw = xw, cy = xy;
+        for (int i = b; i <= carry_idx; ++i) {
+            cw += E[i].x;
+            cy += E[i].y;
+        }
+        *carry = make_longlong2(cw, cy);
+    }
     if (st.cnt_win) {
         for (int i = b; i < e; ++i) {
             const longlong2 v = E[i];
@@ -927,20 +955,28 @@ __device__ __forceinline__ float cnt_of(long long x) { return __int_as_float((in
 // The windows (s, len[k]) of KC durations at one start s.  CHECK = false is
 // the interior, where every window ends at or before bin NB: no clamping, no
 // wrap and no range test.  The KC end points are loaded before any is used.
+// Start range of one window search: starts s in [s_lo, s_hi) of a prefix
+// array whose entry i is held at E[i - off]; end points are clamped to idx_max
+// where they are out of range (their windows are skipped).  The whole period
+// in one array is {0, 0, NB, NB}.
+struct WinRange {
+    int off, s_lo, s_hi, idx_max;
+};
+
 template <int GEOM, bool UNIT, bool CNT, int KC, bool CHECK>
 __device__ __forceinline__ void windows_at(const longlong2* E, int NB, int s, const int (&len)[KC],
-                                           const WinConsts& kc, float (&num)[KC], float (&den)[KC],
-                                           bool (&ok)[KC]) {
-    const longlong2 e0 = E[s];
+                                           const WinConsts& kc, const WinRange& rg,
+                                           float (&num)[KC], float (&den)[KC], bool (&ok)[KC]) {
+    const longlong2 e0 = E[s - rg.off];
     longlong2 e1[KC];
 #pragma unroll
     for (int k = 0; k < KC; ++k) {
         int idx = s + len[k];
         if (CHECK) {
             if (GEOM == ATB_GEOM_FIXED && idx > NB) idx -= NB;
-            idx = min(idx, NB);
+            idx = min(idx, rg.idx_max);
         }
-        e1[k] = E[idx];
+        e1[k] = E[idx - rg.off];
     }
 #pragma unroll
     for (int k = 0; k < KC; ++k) {
@@ -1006,7 +1042,8 @@ __device__ __forceinline__ void window_filter(const float (&num)[KC], const floa
 template <int GEOM, bool UNIT, bool CNT, int KC>
 __device__ __forceinline__ void window_chunk(const longlong2* E, int NB, int nd, int k0,
                                              const int* lens_smem, int tid, int nthreads,
-                                             const WinConsts& kc, Best& best) {
+                                             const WinConsts& kc, const WinRange& rg,
+                                             Best& best) {
     int len[KC];
     int lmax = 0;
 #pragma unroll
@@ -1016,28 +1053,29 @@ __device__ __forceinline__ void window_chunk(const longlong2* E, int NB, int nd,
     }
     // interior starts: s + lmax <= NB (and, with fixed bins, every window
     // shorter than the period)
-    const int s_end = (GEOM == ATB_GEOM_FIXED && lmax >= NB) ? 0 : NB - lmax + 1;
-    // warp-uniform trip count (lanes past NB skip the body), so that the
-    // warp can share its filter bound after every step
+    const int s_end =
+        min(rg.s_hi, (GEOM == ATB_GEOM_FIXED && lmax >= NB) ? 0 : NB - lmax + 1);
+    // warp-uniform trip count (lanes past the range skip the body), so that
+    // the warp can share its filter bound after every step
     const int lane = tid & 31;
-    int s0 = tid - lane;
+    int s0 = rg.s_lo + tid - lane;
     // interior steps (every lane's start is interior): no divergence
     for (; s0 + 31 < s_end; s0 += nthreads) {
         const int s = s0 + lane;
         float num[KC], den[KC];
         bool ok[KC];
-        windows_at<GEOM, UNIT, CNT, KC, false>(E, NB, s, len, kc, num, den, ok);
+        windows_at<GEOM, UNIT, CNT, KC, false>(E, NB, s, len, kc, rg, num, den, ok);
         window_filter<KC>(num, den, ok, s * nd + k0, best);
     }
     // the remaining steps
-    for (; s0 < NB; s0 += nthreads) {
+    for (; s0 < rg.s_hi; s0 += nthreads) {
         const int s = s0 + lane;
         float num[KC], den[KC];
         bool ok[KC];
         if (s < s_end) {
-            windows_at<GEOM, UNIT, CNT, KC, false>(E, NB, s, len, kc, num, den, ok);
-        } else if (s < NB) {
-            windows_at<GEOM, UNIT, CNT, KC, true>(E, NB, s, len, kc, num, den, ok);
+            windows_at<GEOM, UNIT, CNT, KC, false>(E, NB, s, len, kc, rg, num, den, ok);
+        } else if (s < rg.s_hi) {
+            windows_at<GEOM, UNIT, CNT, KC, true>(E, NB, s, len, kc, rg, num, den, ok);
         } else {
 #pragma unroll
             for (int k = 0; k < KC; ++k) {
@@ -1053,19 +1091,23 @@ __device__ __forceinline__ void window_chunk(const longlong2* E, int NB, int nd,
 // All windows of one period over starts tid, tid+nthreads, ...  Durations are
 // taken four at a time (then two, then one): the end points of a chunk are
 // loaded together (instruction-level parallelism with few live registers).
+// `lim0` (>= 0) starts the filter bound: a ratio some window is known to reach.
 template <int GEOM, bool UNIT, bool CNT>
 __device__ Cand window_search(const longlong2* E, int NB, int nd, const int* lens_smem, int tid,
-                              int nthreads, const WinConsts& kc) {
+                              int nthreads, const WinConsts& kc, const WinRange& rg,
+                              float lim0 = 0.0f) {
     Best best;
     best.init();
+    best.lim = lim0;
     int k0 = 0;
     for (; k0 + 4 <= nd; k0 += 4)
-        window_chunk<GEOM, UNIT, CNT, 4>(E, NB, nd, k0, lens_smem, tid, nthreads, kc, best);
+        window_chunk<GEOM, UNIT, CNT, 4>(E, NB, nd, k0, lens_smem, tid, nthreads, kc, rg, best);
     if (nd - k0 >= 2) {
-        window_chunk<GEOM, UNIT, CNT, 2>(E, NB, nd, k0, lens_smem, tid, nthreads, kc, best);
+        window_chunk<GEOM, UNIT, CNT, 2>(E, NB, nd, k0, lens_smem, tid, nthreads, kc, rg, best);
         k0 += 2;
     }
-    if (nd - k0 >= 1) window_chunk<GEOM, UNIT, CNT, 1>(E, NB, nd, k0, lens_smem, tid, nthreads, kc, best);
+    if (nd - k0 >= 1)
+        window_chunk<GEOM, UNIT, CNT, 1>(E, NB, nd, k0, lens_smem, tid, nthreads, kc, rg, best);
     return best.c;
 }
 
@@ -1131,12 +1173,13 @@ __device__ void finalize_period(const SearchArgs& a, GroupSmem& gs, const Team& 
         kc.qw0s = qw0s;
         const int* lens = (GEOM == ATB_GEOM_BINNED) ? gs.dbins : gs.L[tm.id];
         const bool unit = GEOM == ATB_GEOM_FIXED || st.thr_unit;
+        const WinRange rg{0, 0, NB, NB};
         if (cnt)
-            best = unit ? window_search<GEOM, true, true>(E, NB, nd, lens, tm.tid, tm.nthreads, kc)
-                        : window_search<GEOM, false, true>(E, NB, nd, lens, tm.tid, tm.nthreads, kc);
+            best = unit ? window_search<GEOM, true, true>(E, NB, nd, lens, tm.tid, tm.nthreads, kc, rg)
+                        : window_search<GEOM, false, true>(E, NB, nd, lens, tm.tid, tm.nthreads, kc, rg);
         else
-            best = unit ? window_search<GEOM, true, false>(E, NB, nd, lens, tm.tid, tm.nthreads, kc)
-                        : window_search<GEOM, false, false>(E, NB, nd, lens, tm.tid, tm.nthreads, kc);
+            best = unit ? window_search<GEOM, true, false>(E, NB, nd, lens, tm.tid, tm.nthreads, kc, rg)
+                        : window_search<GEOM, false, false>(E, NB, nd, lens, tm.tid, tm.nthreads, kc, rg);
     }
     best = team_best(tm, gs, best);
 
@@ -1191,6 +1234,144 @@ __device__ void finalize_period(const SearchArgs& a, GroupSmem& gs, const Team& 
         if (a.window) a.window[slot] = o_win;
     }
     team_sync(tm);  // per-team scratch (window lengths, scan totals) is reused by the next period
+}
+
+// One astropy-binned period whose NB+1 prefix entries exceed the shared
+// histogram area, searched in bin-range passes through shared memory: pass r
+// folds every point but keeps only slots [lo, lo+W) (lo = r*S, S = W - Lmax,
+// Lmax the longest window), applies the V42 padding copy to the slots it
+// holds, scans them on top of the exact sums of every slot below lo (carried
+// from the previous pass), and searches the windows that start in [lo, lo+S)
+// -- each ends inside the pass.  The prefix values, and therefore every
+// window's score, are the ones the single-pass path computes; the best window
+// over the passes is kept with the same exact comparison, together with its
+// two prefix entries for the final FP64 statistics.  The whole CTA is one team.
+__device__ void run_period_binned_passes(const SearchArgs& a, GroupSmem& gs, longlong2* H,
+                                         const CurveStat& st, long long so, long long n_pad,
+                                         int nd) {
+    const int NB = gs.NBB[0].x;
+    const double P = gs.PIP[0].x;
+    const int os = a.oversample;
+    int Lmax = 0;
+    for (int k = 0; k < nd; ++k) Lmax = max(Lmax, gs.dbins[k]);
+    const int W = a.cap - 2;
+    const int S = W - Lmax;  // >= 1: checked when the group was formed
+    Team tm;
+    tm.id = 0;
+    tm.nwarps = kWarps;
+    tm.nthreads = kBlock;
+    tm.warp0 = 0;
+    tm.tid = threadIdx.x;
+    const bool cnt = st.cnt_win != 0;
+    const double qw0s = ldexp((double)st.qw0, -st.ew);
+    const double wtot = ldexp((double)st.qw_tot, -st.ew);
+    const double ytot = ldexp((double)st.qy_tot, -st.ey);
+    const float fN = (float)st.n_cnt;
+    WinConsts kc;
+    kc.wtot = wtot;
+    kc.ytot = ytot;
+    kc.c1 = cnt ? (float)(ytot / (double)fN) : (float)(ytot / wtot);
+    kc.fN = fN;
+    kc.thr = ldexp(1e-15, st.s_w - st.ew);
+    kc.qw0s = qw0s;
+    const bool unit = st.thr_unit != 0;
+    if (threadIdx.x == 0) {
+        gs.mp_num = -1.0f;
+        gs.mp_den = 1.0f;
+        gs.mp_key = 0x7fffffff;
+        gs.carry = make_longlong2(0, 0);
+    }
+    uint4* HU = reinterpret_cast<uint4*>(H);
+    for (int lo = 0; lo < NB; lo += S) {
+        for (int i = threadIdx.x; i < W; i += kBlock) H[i] = make_longlong2(0, 0);
+        __syncthreads();
+        if (st.packmode == kPackTight)
+            fold_group<ATB_GEOM_BINNED, false, kPackTight, true>(a, gs, HU, so, n_pad, st, lo, W);
+        else if (st.packmode == kPackCount)
+            fold_group<ATB_GEOM_BINNED, false, kPackCount, true>(a, gs, HU, so, n_pad, st, lo, W);
+        else
+            fold_group<ATB_GEOM_BINNED, false, kPackSplit, true>(a, gs, HU, so, n_pad, st, lo, W);
+        __syncthreads();
+        // padding copy, vbls_v42_parity.cu:78-80: bins 1..os (saved by the
+        // first pass) replace bins NB-os..NB-1 wherever a pass holds them
+        if (lo == 0 && threadIdx.x < os) gs.pad_save[threadIdx.x] = load_components(HU, 1 + threadIdx.x);
+        __syncthreads();
+        if (threadIdx.x < os) {
+            const int j = NB - os + threadIdx.x - lo;
+            if (j >= 0 && j < W) store_components(HU, j, gs.pad_save[threadIdx.x]);
+        }
+        __syncthreads();
+        const int M = min(W, NB + 1 - lo);
+        const longlong2 c0 = gs.carry;
+        __syncthreads();
+        team_scan(tm, gs, H, M, st, c0.x, c0.y, S - 1 < M ? S - 1 : -1, &gs.carry);
+        Cand best{-1.0f, 1.0f, 0x7fffffff};
+        if (wtot > 0.0) {
+            const WinRange rg{lo, lo, min(lo + S, NB), min(NB, lo + W - 1)};
+            const float lim0 = gs.mp_key != 0x7fffffff
+                                   ? __fmul_rn(__fdiv_rn(gs.mp_num, gs.mp_den), 0.99999904632568359375f)
+                                   : 0.0f;
+            if (cnt)
+                best = unit ? window_search<ATB_GEOM_BINNED, true, true>(H, NB, nd, gs.dbins, tm.tid,
+                                                                         tm.nthreads, kc, rg, lim0)
+                            : window_search<ATB_GEOM_BINNED, false, true>(H, NB, nd, gs.dbins, tm.tid,
+                                                                          tm.nthreads, kc, rg, lim0);
+            else
+                best = unit ? window_search<ATB_GEOM_BINNED, true, false>(H, NB, nd, gs.dbins, tm.tid,
+                                                                          tm.nthreads, kc, rg, lim0)
+                            : window_search<ATB_GEOM_BINNED, false, false>(H, NB, nd, gs.dbins, tm.tid,
+                                                                           tm.nthreads, kc, rg, lim0);
+        }
+        best = team_best(tm, gs, best);
+        if (threadIdx.x == 0 && best.key != 0x7fffffff &&
+            cand_better(best.num, best.den, best.key, gs.mp_num, gs.mp_den, gs.mp_key)) {
+            const int s = best.key / nd, k = best.key % nd;
+            gs.mp_num = best.num;
+            gs.mp_den = best.den;
+            gs.mp_key = best.key;
+            gs.mp_e0 = H[s - lo];
+            gs.mp_e1 = H[s + gs.dbins[k] - lo];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const long long slot = gs.slot[0];
+        float o_pw = 0.0f, o_dep = 0.0f, o_de = 0.0f, o_dur = 0.0f;
+        double o_t0 = 0.0;
+        int o_win = -1;
+        if (gs.mp_key != 0x7fffffff) {
+            const int s = gs.mp_key / nd, k = gs.mp_key % nd;
+            const int dd = gs.dbins[k];
+            auto pw_of = [&](const longlong2 e) {
+                return cnt ? (double)cnt_of(e.x) * qw0s : ll_as_d(e.x);
+            };
+            const double dw = pw_of(gs.mp_e1) - pw_of(gs.mp_e0);
+            const double dy = ll_as_d(gs.mp_e1.y) - ll_as_d(gs.mp_e0.y);
+            const double durv = (double)dd * st.bin_dur;
+            o_dur = (float)durv;
+            o_t0 = fmod((double)s * st.bin_dur + 0.5 * durv + st.t_start, P);
+            double pw, dep, de;
+            window_stats(dw, dy, wtot, ytot, st.s_w - st.ew, st.s_y - st.ey, a.objective, &pw, &dep,
+                         &de);
+            o_pw = (float)pw;
+            o_dep = (float)dep;
+            o_de = (float)de;
+            o_win = gs.mp_key;
+        }
+        if (a.best_key && o_win >= 0) {
+            const unsigned long long key =
+                ((unsigned long long)__float_as_uint(o_pw) << 32) |
+                (unsigned long long)(0xffffffffu - (unsigned)(slot - a.out_beg[gs.curve]));
+            atomicMax(a.best_key + gs.curve, key);
+        }
+        if (a.power) a.power[slot] = o_pw;
+        if (a.depth) a.depth[slot] = o_dep;
+        if (a.depth_err) a.depth_err[slot] = o_de;
+        if (a.t0) a.t0[slot] = o_t0;
+        if (a.duration) a.duration[slot] = o_dur;
+        if (a.window) a.window[slot] = o_win;
+    }
+    __syncthreads();
 }
 
 template <int GEOM, bool GLOB>
@@ -1300,10 +1481,18 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) search_kernel(const Search
                 gs.G = g;
                 gs.total = base;
                 gs.glob = base > a.cap ? 1 : 0;
+                if (gs.glob && GEOM == ATB_GEOM_BINNED && a.oversample <= kMpPadMax) {
+                    int lmax = 0;
+                    for (int k = 0; k < nd; ++k) lmax = max(lmax, gs.dbins[k]);
+                    // a pass must hold the windows of at least 64 starts
+                    if (a.cap - 2 - lmax >= 64) gs.glob = 2;
+                }
                 gs.safe_floor = (st.dt_absmax * ipmax < 1.0e15) ? 1 : 0;
             }
             __syncthreads();
-            if (gs.glob) {
+            if (gs.glob == 2) {
+                run_period_binned_passes(a, gs, s_hist, st, so, n_pad, nd);
+            } else if (gs.glob) {
                 run_group<GEOM, true>(a, gs, a.ghist + (long long)blockIdx.x * a.ghist_stride, st,
                                       so, n_pad, nd);
             } else {

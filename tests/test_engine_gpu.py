@@ -138,8 +138,9 @@ def test_binned_bit_exact_reference_cap(engine):
 
 
 def test_binned_global_histogram_fallback(engine):
-    """Periods whose bin count exceeds shared memory use the global-memory
-    histograms; results stay bit-exact (here up to ~60k bins)."""
+    """Periods whose bin count exceeds shared memory are searched in bin-range
+    passes through shared memory; results stay bit-exact (here up to ~60k
+    bins)."""
     rng = np.random.default_rng(4)
     t = np.sort(rng.uniform(0, 60.0, 4000))
     y = R.inject_box(t, 1.0 + rng.normal(0, 1e-3, t.size), 11.0, 3.0, 0.05, 3e-3)
@@ -149,6 +150,33 @@ def test_binned_global_histogram_fallback(engine):
     g = run(engine, t, y, w, periods, durs, cfg_binned())
     o = O.eng_binned(t, y, w, periods, durs)
     assert_bit_exact(g, o, "fallback")
+
+
+@pytest.mark.parametrize("weighted", [False, True])
+def test_binned_bin_range_passes_long_windows(engine, weighted):
+    """Bin-range passes with long windows (up to 800 bins), a transit near the
+    end of the period (the V42 padding bins), a grid mixing periods that fit
+    shared memory with ones that do not, and a bin cap that does not bind:
+    bit-exact against the oracle."""
+    rng = np.random.default_rng(14 + weighted)
+    t = np.sort(rng.uniform(0, 356.0, 20000)) + 1500.0
+    y = R.inject_box(t, 1.0 + rng.normal(0, 1e-3, t.size), 97.3, 1590.0, 0.3, 2e-3)
+    w = (rng.uniform(2e5, 1e6, t.size) if weighted else np.full(t.size, 4e5)).astype(np.float32)
+    periods = np.concatenate([np.geomspace(0.7, 13.0, 40), np.geomspace(14.0, 170.0, 30)])
+    durs = np.array([0.01, 0.05, 0.2, 0.4, 0.8])  # bin 0.001 d: windows of 10..800 bins
+    for mb in (None, 10 ** 6):
+        g = run(engine, t, y, w, periods, durs, cfg_binned("likelihood", max_bins=mb))
+        o = O.eng_binned(t, y, w, periods, durs, objective="likelihood", max_bins=mb or 0)
+        assert_bit_exact(g, o, f"passes w={weighted} mb={mb}")
+
+
+def test_fixed_global_histogram_fallback(engine):
+    """Fixed bins beyond one CTA's shared memory use per-CTA global
+    histograms; bit-exact."""
+    t, f, _, periods, durs = R.astropy_parity_recipe()
+    g = run(engine, t, f, None, periods[::10], durs, cfg_fixed(20000))
+    o = O.eng_fixed(t, f, None, periods[::10], durs, n_bins=20000)
+    assert_bit_exact(g, o, "fixed-glob")
 
 
 @pytest.mark.parametrize("n_bins", [200, 500, 1024, 3000])
