@@ -52,9 +52,13 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--workload", default="uniform", choices=["uniform", "mixed"],
+    ap.add_argument("--workload", default="uniform", choices=["uniform", "mixed", "precision"],
                     help="uniform: the 4096 x 15000 batch (default); mixed: the uneven batch "
-                         "(N log-U[1e3, 2e5], 1-13 sectors, per-curve period grids)")
+                         "(N log-U[1e3, 2e5], 1-13 sectors, per-curve period grids); "
+                         "precision: 512 x 200000 points over ~356 d, 100000 periods "
+                         "0.5-150 d (errors against the FP64 oracle on a sample)")
+    ap.add_argument("--precision-sample", type=int, default=2,
+                    help="precision workload: curves checked against the FP64 oracle")
     ap.add_argument("--method", default="parity", choices=["parity", "fast"])
     ap.add_argument("--curves", type=int, default=None,
                     help="curves per GPU (default 4096 uniform, 8192 mixed)")
@@ -69,7 +73,7 @@ def parse():
     ap.add_argument("--no-serving", action="store_true")
     args = ap.parse_args()
     if args.curves is None:
-        args.curves = 4096 if args.workload == "uniform" else 8192
+        args.curves = {"uniform": 4096, "mixed": 8192, "precision": 512}[args.workload]
     return args
 
 
@@ -81,6 +85,22 @@ def search_config(args):
 
 
 def workload_config(args, n_gpus):
+    if args.workload == "precision":
+        return {
+            "workload": (f"precision stress: {args.curves} curves per GPU x 200000 float32 points "
+                         "(2-min cadence, 13 sectors, ~356 d, t offset U[1300, 2700] BTJD, "
+                         "sigma 5e-4, one 5e-4-deep transit), 100000 frequency-uniform periods "
+                         "0.5-150 d, 8 durations 0.02-0.30 d, "
+                         + ("fixed 200 bins, fast score" if args.method == "fast" else
+                            "astropy-binned (oversample 10), likelihood objective")),
+            "n_curves_per_gpu": args.curves, "method": args.method,
+            "objective": "fast" if args.method == "fast" else "likelihood",
+            "precision": "FP64 fold, int64 fixed-point bin sums, FP32 window search, FP64 winner",
+            "l2": "no flush: staged inputs per GPU are about 1.6 GB (L2 is 126 MB)",
+            "parallelism": f"dp{n_gpus} (curves sharded across GPUs, no data-path collective)",
+            "seed": "precision_curve(default_rng(3000+rank))",
+            "launch": "CUDA graph replay of the plan (stage, persistent search, best peak)",
+        }
     if args.workload == "mixed":
         return {
             "workload": (f"uneven batch: {args.curves} curves per GPU, N log-U[1e3, 2e5] float32 "
@@ -181,6 +201,13 @@ def make_workload(args, rank):
     """(t, y, w, periods, durations): arrays [curves, n] and one shared grid
     for the uniform batch, lists of per-curve arrays for the mixed batch."""
     import recipes as R
+    if args.workload == "precision":
+        rng = np.random.default_rng(3000 + rank)
+        cs = [R.precision_curve(rng) for _ in range(args.curves)]
+        t = np.stack([c[0] for c in cs])
+        y = np.stack([c[1] for c in cs])
+        w = np.stack([(1.0 / (c[2].astype(np.float64) ** 2)).astype(np.float32) for c in cs])
+        return t, y, w, R.precision_periods(), list(R.C3_DURATIONS)
     if args.workload == "mixed":
         cs = R.mixed_batch(args.curves, seed=2000 + rank)
         t = [c[0] for c in cs]
@@ -253,6 +280,36 @@ def run_reference(args):
         "gpu_launches": 0,
     }
     print(json.dumps(line), flush=True)
+
+
+def precision_report(args, sess, t, y, w, periods, durs):
+    """Errors of the engine against the FP64 restatement of the reference on
+    the first `--precision-sample` curves (every period): relative power error
+    (max, median), and the best peak's period and transit-time differences."""
+    from oracle import oracle as O
+    gp = sess.host_out["power"].numpy()
+    gt0 = sess.host_out["t0"].numpy()
+    ob = sess.batch.out_begin
+    rel, dper, dt0 = [], [], []
+    for c in range(min(args.precision_sample, len(t))):
+        if args.method == "fast":
+            o = O.ref_fixed(t[c], y[c], w[c], periods, durs, n_bins=200)
+        else:
+            o = O.ref_binned(t[c], y[c], w[c], periods, durs, oversample=OVERSAMPLE,
+                             objective="likelihood")
+        n = len(o["power"])
+        g = gp[ob[c]:ob[c] + n]
+        rel.append(np.abs(g - o["power"]) / np.maximum(o["power"], 1e-30))
+        bg, bo = int(np.argmax(g)), int(np.argmax(o["power"]))
+        dper.append(abs(periods[bg] - periods[bo]))
+        dt0.append(abs(gt0[ob[c] + bg] - o["t0"][bo]))
+    r = np.concatenate(rel)
+    return {"curves": len(rel), "periods_per_curve": len(periods),
+            "max_rel_power_err": float(r.max()), "median_rel_power_err": float(np.median(r)),
+            "best_period_abs_diff_d": [float(x) for x in dper],
+            "best_t0_abs_diff_d": [float(x) for x in dt0],
+            "reference": "oracle FP64 restatement of the reference kernel (fold, sums, windows "
+                         "all FP64)"}
 
 
 def run_serving(args, device):
@@ -410,7 +467,9 @@ def main():
         },
         "clocks": clocks.summary() if rank == 0 else None,
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and args.workload == "precision":
+        line["precision_vs_fp64"] = precision_report(args, sess, t, y, w, periods, durs)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload != "precision":
         rate, cores, sample, outs, _ = cpu_reference(t, y, w, periods, durs, args.method,
                                                      args.cpu_seconds)
         gp = sess.host_out["power"].numpy()

@@ -192,3 +192,30 @@ def mixed_batch(n_curves=8192, seed=2, max_points=None):
             n = min(n, max_points)
         out.append(mixed_curve(rng, n_sec, cad, n, n_per))
     return out
+
+
+def precision_curve(rng, n=200_000, n_sec=13, sigma=5e-4):
+    """Precision-stress curve: t offset U[1300, 2700] BTJD, 13 concatenated
+    sectors (~356 d) at 2-min cadence with mid-sector gaps, n points, white
+    noise sigma and one box transit (P U[0.5, 40] d, duration U[0.05, 0.3] d,
+    depth 5e-4).  Returns (t, y float32, dy float32, (P, t0, duration))."""
+    t_offset = rng.uniform(1300.0, 2700.0)
+    grid = []
+    for s in range(n_sec):
+        g = np.arange(0.0, SECTOR_DAYS, CADENCE_2MIN)
+        lo, hi = 0.5 * (SECTOR_DAYS - 1.0), 0.5 * (SECTOR_DAYS + 1.0)
+        grid.append(t_offset + s * SECTOR_DAYS + g[(g < lo) | (g >= hi)])
+    grid = np.concatenate(grid)
+    t = grid[np.sort(rng.choice(grid.size, size=min(n, grid.size), replace=False))]
+    P, dur = rng.uniform(0.5, 40.0), rng.uniform(0.05, 0.3)
+    t0 = t[0] + rng.uniform(0.0, P)
+    y = inject_box(t, 1.0 + rng.normal(0.0, sigma, t.size), P, t0, dur, 5e-4)
+    return t, y.astype(np.float32), np.full(t.size, sigma, np.float32), (P, t0, dur)
+
+
+def precision_periods(n=100_000, pmin=0.5, pmax=150.0):
+    """Frequency-uniform grid over [pmin, pmax] (largest period first)."""
+    return 1.0 / np.linspace(1.0 / pmin, 1.0 / pmax, n)[::-1]
+
+
+C3_DURATIONS = np.geomspace(0.02, 0.3, 8)
