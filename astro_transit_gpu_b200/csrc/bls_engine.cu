@@ -181,6 +181,7 @@ struct SearchArgs {
     unsigned long long* tile_counter;
     int* status;
     unsigned long long* best_key;  // winner-take-all per-curve records (or NULL)
+    int tile_p;                    // periods per work-queue tile (1..kTileP)
 };
 
 // ----------------------------------------------------------------------------
@@ -1423,8 +1424,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) search_kernel(const Search
                 }
                 const int c = a.order[lo];
                 gs.curve = c;
-                gs.pb = (tile - a.tile_off[lo]) * kTileP;
-                gs.pe = min(gs.pb + kTileP, a.per_cnt[c]);
+                gs.pb = (tile - a.tile_off[lo]) * a.tile_p;
+                gs.pe = min(gs.pb + a.tile_p, a.per_cnt[c]);
             }
         }
         __syncthreads();
@@ -1949,9 +1950,24 @@ int plan_create(atb_handle* h, const atb_params* prm, const atb_batch* b, const 
         const double cy = (double)(pt_off[y + 1] - pt_off[y] + 64) * (double)per_cnt[y];
         return cx > cy;
     });
+    // periods per tile: as requested, else the largest power of two up to
+    // kTileP that still gives every resident CTA about four tiles (a small
+    // batch -- one curve of a few thousand periods -- otherwise leaves most
+    // SMs idle)
+    int tile_p = prm->tile_periods;
+    if (tile_p < 1 || tile_p > kTileP) {
+        const long long slots = 4LL * h->n_sm * kMinBlocks;
+        tile_p = kTileP;
+        while (tile_p > 8) {
+            long long tiles = 0;
+            for (int c = 0; c < nc; ++c) tiles += (per_cnt[c] + tile_p - 1) / tile_p;
+            if (tiles >= slots) break;
+            tile_p /= 2;
+        }
+    }
     tile_off[0] = 0;
     for (int j = 0; j < nc; ++j)
-        tile_off[j + 1] = tile_off[j] + (per_cnt[order[j]] + kTileP - 1) / kTileP;
+        tile_off[j + 1] = tile_off[j] + (per_cnt[order[j]] + tile_p - 1) / tile_p;
 
     ATB_CUDA(h, cudaSetDevice(h->device));
     atb_plan* p = new atb_plan();
@@ -2103,6 +2119,7 @@ int plan_create(atb_handle* h, const atb_params* prm, const atb_batch* b, const 
     qa.dbins = d_dbins;
     qa.power = o->power;
     qa.best_key = reinterpret_cast<unsigned long long*>(o->best_key);
+    qa.tile_p = tile_p;
     qa.depth = o->depth;
     qa.depth_err = o->depth_err;
     qa.t0 = o->t0;
@@ -2670,6 +2687,7 @@ extern "C" int atb_search_curve_static(const atb_params* prm, const double* t, c
     qa.ghist = nullptr;  // never reached: every period fits shared memory (checked above)
     qa.ghist_stride = 0;
     qa.tile_counter = &m->tile_counter;
+    qa.tile_p = kTileP;
     qa.status = &m->status;
     int occ = 1;
     if (prm->geometry == ATB_GEOM_BINNED)

@@ -31,26 +31,31 @@ class SearchConfig:
                for method="parity"
     max_bins   None = no cap; an int reproduces the reference's cap
                n_bins = min(n_bins, max_bins-1) (vbls_v42_parity.cu:46-47)
+    tile_periods  periods per work-queue tile (1..64); 0 = chosen from the
+               batch size, or the value BLSEngine.autotune found for this
+               kind of batch.  Results never depend on it.
     """
     method: str = "parity"
     objective: Optional[str] = None
     n_bins: int = 200
     oversample: int = 10
     max_bins: Optional[int] = None
+    tile_periods: int = 0
 
     def params(self) -> N.Params:
         if self.method == "fast":
             obj = self.objective or "fast"
             if obj != "fast":
                 raise ValueError("method='fast' uses the reference's fast score")
-            return N.Params(N.GEOM_FIXED, N.OBJ_FAST, int(self.n_bins), int(self.oversample), 0, 0)
+            return N.Params(N.GEOM_FIXED, N.OBJ_FAST, int(self.n_bins), int(self.oversample), 0,
+                            int(self.tile_periods))
         if self.method == "parity":
             obj = self.objective or "snr"
             if obj not in ("snr", "likelihood"):
                 raise ValueError("method='parity' supports objective 'snr' or 'likelihood'")
             mb = 0 if self.max_bins is None else int(self.max_bins)
             return N.Params(N.GEOM_BINNED, N.OBJECTIVES[obj], int(self.n_bins),
-                            int(self.oversample), mb, 0)
+                            int(self.oversample), mb, int(self.tile_periods))
         raise ValueError(f"unknown method {self.method!r} (expected 'fast' or 'parity')")
 
 
@@ -308,6 +313,8 @@ class BLSEngine:
                            torch.device(device).index or 0)
         self.device = dev
         self.handle = N.Handle(dev.index)
+        self._tuned: Dict[tuple, int] = {}  # tune_key -> tile periods (autotune)
+        self.last_tune: Dict[int, float] = {}
 
     @classmethod
     def get(cls, device=None) -> "BLSEngine":
@@ -343,11 +350,48 @@ class BLSEngine:
                                              device=batch.device)
         return out
 
+    @staticmethod
+    def tune_key(batch: CurveBatch, config: SearchConfig):
+        """The kind of batch a tuned setting applies to: method, and the
+        powers of two of the curve count, mean points and mean periods."""
+        nc = max(batch.n_curves, 1)
+        pts = float(batch.point_offset[-1]) / nc
+        per = float(np.sum(batch.period_count)) / nc
+        b = lambda v: int(np.log2(max(v, 1.0)))  # noqa: E731
+        return (config.method, b(nc), b(pts), b(per))
+
+    def autotune(self, batch: CurveBatch, config: SearchConfig,
+                 candidates: Sequence[int] = (8, 16, 32, 64), repeats: int = 2) -> int:
+        """Time the search kernel on `batch` for each tile size in `candidates`
+        (results are identical for all), keep the fastest for this kind of
+        batch (``tune_key``) and return it; later plans with
+        ``tile_periods == 0`` use it."""
+        times = {}
+        for tp in candidates:
+            cfg = SearchConfig(config.method, config.objective, config.n_bins, config.oversample,
+                               config.max_bins, int(tp))
+            plan = SearchPlan(self, batch, cfg, self.allocate_outputs(batch))
+            try:
+                plan.execute()
+                torch.cuda.synchronize(batch.device)
+                times[int(tp)] = min(plan.profile()["search"] for _ in range(max(1, repeats)))
+            finally:
+                plan.close()
+        best = min(times, key=times.get)
+        self._tuned[self.tune_key(batch, config)] = best
+        self.last_tune = times
+        return best
+
     def plan(self, batch: CurveBatch, config: SearchConfig,
              outputs: Optional[Dict[str, torch.Tensor]] = None,
              stream: Optional[torch.cuda.Stream] = None) -> SearchPlan:
         if outputs is None:
             outputs = self.allocate_outputs(batch)
+        if config.tile_periods == 0:
+            tp = self._tuned.get(self.tune_key(batch, config))
+            if tp is not None:
+                config = SearchConfig(config.method, config.objective, config.n_bins,
+                                      config.oversample, config.max_bins, tp)
         return SearchPlan(self, batch, config, outputs, stream)
 
     def screen(self, batch: CurveBatch, config: SearchConfig,

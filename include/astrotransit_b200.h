@@ -58,7 +58,8 @@ typedef struct {
     int32_t oversample; /* BINNED: bins per minimum duration (reference default 10, api.py:76) */
     int32_t max_bins;   /* BINNED: 0 = no cap; >0 reproduces the reference's bin cap
                            n_bins = min(n_bins, max_bins-1), vbls_v42_parity.cu:46-47 */
-    int32_t reserved;
+    int32_t tile_periods; /* periods per work-queue tile, 1..64; 0 = chosen from the batch
+                             size (no reference counterpart; results do not depend on it) */
 } atb_params;
 
 /*

@@ -404,3 +404,28 @@ def test_screen_equals_full_search_at_its_best_period(engine, method):
         assert scr["period"][c] == ps[c][bi]
         for k in FIELDS:
             assert scr[k][c] == full[k][g], (c, k)
+
+
+# ------------------------------------------------------------ autotuning ---
+
+def test_tile_size_never_changes_results_and_autotune_picks_one(engine):
+    """Every tile size (periods per work-queue tile) gives bit-identical
+    outputs; the autotuner times the candidates and later plans of the same
+    kind of batch use the winner."""
+    from astro_transit_gpu_b200.engine import CurveBatch, SearchConfig
+    t, y, dy, _ = R.uniform_batch(n_curves=3, n=3000, seed=17)
+    per = [np.geomspace(0.5, 13.7, n) for n in (700, 1500, 333)]
+    b = CurveBatch.from_arrays(list(t), list(y), list(dy), periods=per,
+                               durations=R.C0_DURATIONS, device=engine.device)
+    ref = None
+    for tp in (0, 1, 7, 8, 64):
+        cfg = SearchConfig("parity", objective="likelihood", tile_periods=tp)
+        out = {k: v.cpu().numpy() for k, v in engine.search(b, cfg).items()}
+        if ref is None:
+            ref = out
+        for k in ref:
+            assert np.array_equal(out[k], ref[k]), (tp, k)
+    cfg = SearchConfig("parity", objective="likelihood")
+    best = engine.autotune(b, cfg, candidates=(8, 64))
+    assert best in (8, 64) and set(engine.last_tune) == {8, 64}
+    assert engine._tuned[engine.tune_key(b, cfg)] == best
