@@ -756,7 +756,45 @@ __device__ void window_stats(double dw, double dy, double wtot, double ytot, int
     *derr = de;
 }
 
-// Inclusive scan of the raw histogram entries H[0..M) in place.  Pass 1
+// Exact sums (W, Y) of raw histogram entry i in layout MODE: the words the
+// layout uses are read directly (component c of entry i is word c ^ rot(i),
+// at byte offset 4c ^ (((i - 1) >> 1) & 12) in the entry).
+template <int MODE>
+__device__ __forceinline__ void entry_sums_m(const longlong2* E, int i, const CurveStat& st,
+                                             long long& w, long long& y) {
+    const unsigned* ent = reinterpret_cast<const unsigned*>(E + i);
+    const unsigned r = slot_rot(i);
+    const unsigned x = ent[0u ^ r];
+    if (MODE == kPackTight) {
+        const unsigned z = ent[2u ^ r];
+        w = (long long)(x >> st.cshift);
+        y = (long long)(int)z * (1LL << st.lobits) + (long long)(x & ((1u << st.cshift) - 1u));
+    } else {
+        const unsigned z = ent[2u ^ r], v = ent[3u ^ r];
+        w = MODE == kPackCount ? (long long)x
+                               : (long long)ent[1u ^ r] * (1LL << st.lobits) + (long long)x;
+        y = (long long)(int)v * (1LL << st.lobits) + (long long)z;
+    }
+    if (MODE != kPackSplit && !st.cnt_win) w *= (long long)st.qw0;
+}
+
+// Pass 1 of the scan for layout MODE: decode entries [b, e) once, write
+// their exact int64 sums back in place, return the segment's totals.
+template <int MODE>
+__device__ __forceinline__ void scan_decode(longlong2* E, int b, int e, const CurveStat& st,
+                                            long long& sw, long long& sy) {
+    sw = 0;
+    sy = 0;
+    for (int i = b; i < e; ++i) {
+        long long w, y;
+        entry_sums_m<MODE>(E, i, st, w, y);
+        E[i] = make_longlong2(w, y);
+        sw += w;
+        sy += y;
+    }
+}
+
+// Inclusive scan of the raw histogram entries E[0..M) in place.  Pass 1
 // decodes each entry's split 32-bit words once into exact int64 sums (W, Y)
 // and writes them back; pass 2 adds the running sums and writes exact values:
 // the flux sum as FP64 scaled by 2^-ey, and the weight sum as FP64 scaled by
@@ -764,20 +802,6 @@ __device__ void window_stats(double dw, double dy, double wtot, double ytot, int
 // word (|sum| < 2^53 and counts < 2^24, so every conversion is exact).
 // Threads own contiguous segments of odd length, so the 16-byte entries a
 // warp touches in one step fall in distinct bank groups.
-__device__ __forceinline__ void entry_sums(const uint4* R, int i, const CurveStat& st, long long& w,
-                                           long long& y) {
-    const uint4 e = load_components(R, i);
-    if (st.packmode == kPackTight) {
-        w = (long long)(e.x >> st.cshift);
-        y = (long long)(int)e.z * (1LL << st.lobits) + (long long)(e.x & ((1u << st.cshift) - 1u));
-    } else {
-        w = st.packmode == kPackCount ? (long long)e.x
-                                      : (long long)e.y * (1LL << st.lobits) + (long long)e.x;
-        y = (long long)(int)e.w * (1LL << st.lobits) + (long long)e.z;
-    }
-    if (st.packmode != kPackSplit && !st.cnt_win) w *= (long long)st.qw0;
-}
-
 // cw0, cy0: exact sums added to every prefix (the bins below E[0]); the
 // thread holding entry carry_idx stores that entry's exact prefix in *carry.
 __device__ void team_scan(const Team& tm, GroupSmem& gs, longlong2* E, int M, const CurveStat& st,
@@ -787,15 +811,13 @@ __device__ void team_scan(const Team& tm, GroupSmem& gs, longlong2* E, int M, co
     seg |= 1;
     const int b = min(M, tm.tid * seg);
     const int e = min(M, b + seg);
-    const uint4* R = reinterpret_cast<const uint4*>(E);
-    long long sw = 0, sy = 0;
-    for (int i = b; i < e; ++i) {
-        long long w, y;
-        entry_sums(R, i, st, w, y);
-        E[i] = make_longlong2(w, y);
-        sw += w;
-        sy += y;
-    }
+    long long sw, sy;
+    if (st.packmode == kPackTight)
+        scan_decode<kPackTight>(E, b, e, st, sw, sy);
+    else if (st.packmode == kPackCount)
+        scan_decode<kPackCount>(E, b, e, st, sw, sy);
+    else
+        scan_decode<kPackSplit>(E, b, e, st, sw, sy);
     const int lane = threadIdx.x & 31;
     long long iw = sw, iy = sy;
 #pragma unroll
