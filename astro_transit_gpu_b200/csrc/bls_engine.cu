@@ -64,7 +64,7 @@ constexpr int kMaxG = 64;              // periods per shared-memory group
 constexpr int kMaxDur = 32;            // durations per curve
 constexpr int kStageAlign = 32;        // staged curves start at multiples of 32 points
 constexpr int kStageBlock = 256;
-constexpr double kMagicRound = 4503599627370496.0;  // 2^52: x + 2^52 (rz) truncates x in [0, 2^31)
+constexpr double kMagicSlot = 4503599627370497.0;   // 2^52 + 1: x + C (rz) = 2^52 + int(x) + 1, x in (-1, 2^31 - 1)
 constexpr double kMagicFloor = 6755399441055744.0;  // 1.5*2^52: (m + C)(rd) - C = floor(m), |m| < 2^50
 
 // Histogram word layouts (per curve):
@@ -131,8 +131,8 @@ struct StageArgs {
     const float* w;
     const double* durations;
     double* sdt;
-    int* sqw;
-    int* sqy;
+    int* sqw;  // q_w per point, or the fold's first word (tight, count layouts)
+    int* sqy;  // q_y per point, or the fold's flux word (tight layout)
     CurveStat* stats;
     int* dbins;  // [n_curves * kMaxDur]
     int oversample;
@@ -166,7 +166,7 @@ struct SearchArgs {
     const double* periods;
     const double* durations;
     const double* sdt;
-    const int* sqw;
+    const int* sqw;  // as StageArgs
     const int* sqy;
     const CurveStat* stats;
     const int* dbins;
@@ -204,10 +204,12 @@ __device__ __forceinline__ double floor_magic(double m) {
     return __dadd_rn(__dadd_rd(m, kMagicFloor), -kMagicFloor);
 }
 
-// trunc(x) for x in (-1, 2^31) as an int, with one full-rate FP64 addition;
-// x in (-1, 0) yields a negative value (callers clamp at 0, as int(x) = 0 there)
-__device__ __forceinline__ int trunc_magic(double x) {
-    return __double2loint(__dadd_rz(x, kMagicRound));
+// int(x) + 1 (C truncation toward zero) for x in (-1, 2^31 - 1), with one
+// full-rate FP64 addition: the sum lies in [2^52, 2^53), where the spacing of
+// doubles is 1, so rounding toward zero leaves 2^52 + int(x) + 1, whose low
+// word is the result (0 for x in (-1, 0)).
+__device__ __forceinline__ int trunc1_magic(double x) {
+    return __double2loint(__dadd_rz(x, kMagicSlot));
 }
 
 __device__ __forceinline__ double ll_as_d(long long v) { return __longlong_as_double(v); }
@@ -427,7 +429,13 @@ __global__ void __launch_bounds__(kStageBlock) stage_kernel(const StageArgs a) {
     vmax = block_max_d(vmax, shd);
     const int s_y = q_scale(vmax, qbits_y);
 
-    // pass 4: staged arrays (padded with zero-weight points) and totals
+    // pass 4: staged arrays (padded with zero-weight points) and totals.
+    // Uniform-weight layouts stage the fold's words (see fold_group):
+    //   tight  x = (q_w != 0) << cshift | (q_y & lomask), z = q_y >> lobits
+    //   count  x = (q_w != 0), and q_y as is
+    //   split  q_w and q_y as they are
+    const int lob = packmode == kPackTight ? 32 - 2 * tight_bits : curve_lobits(n);
+    const int csh = 32 - tight_bits;
     long long qw_tot = 0, qy_tot = 0, qy_abs = 0;
     for (long long i = threadIdx.x; i < n_pad; i += kStageBlock) {
         double d = 0.0;
@@ -438,9 +446,16 @@ __global__ void __launch_bounds__(kStageBlock) stage_kernel(const StageArgs a) {
             qb = (int)__double2ll_rn(ldexp(wi * ((double)y[i] - shift), s_y));
             d = t[i] - t_start;
         }
+        int sa = qa, sb = qb;
+        if (packmode == kPackTight) {
+            sa = (int)((qa != 0 ? (1u << csh) : 0u) + ((unsigned)qb & ((1u << lob) - 1u)));
+            sb = qb >> lob;
+        } else if (packmode == kPackCount) {
+            sa = qa != 0 ? 1 : 0;
+        }
         a.sdt[so + i] = d;
-        a.sqw[so + i] = qa;
-        a.sqy[so + i] = qb;
+        a.sqw[so + i] = sa;
+        a.sqy[so + i] = sb;
         qw_tot += qa;
         qy_tot += qb;
         qy_abs += qb < 0 ? -(long long)qb : (long long)qb;
@@ -505,10 +520,9 @@ __device__ __forceinline__ void red_shared_u32(unsigned addr, unsigned v) {
 // Histogram entry of slot s: four 32-bit words -- weight sums split at
 // `lobits` (x, y; x = point count when weights are uniform) and flux sums
 // split the same way (z, w).  Component c is stored in word c ^ rot(s),
-// rot(s) = ((s - 1) >> 3) & 3, so that for a fixed component consecutive
-// slots cycle through all 32 banks (a plain 16-byte layout would use only 8).
-// The fold addresses slots as 1 + t (t = slot - 1), hence the offset.
-__device__ __forceinline__ unsigned slot_rot(int s) { return ((unsigned)(s - 1) >> 3) & 3u; }
+// rot(s) = (s >> 3) & 3, so that for a fixed component consecutive slots
+// cycle through all 32 banks (a plain 16-byte layout would use only 8).
+__device__ __forceinline__ unsigned slot_rot(int s) { return ((unsigned)s >> 3) & 3u; }
 
 __device__ __forceinline__ uint4 load_components(const uint4* H, int s) {
     uint4 e = H[s];
@@ -522,6 +536,10 @@ __device__ __forceinline__ uint4 load_components(const uint4* H, int s) {
         e.x = e.z; e.y = e.w; e.z = t0; e.w = t1;
     }
     return e;
+}
+
+__device__ __forceinline__ uint4 add_words(uint4 u, uint4 v) {
+    return make_uint4(u.x + v.x, u.y + v.y, u.z + v.z, u.w + v.w);
 }
 
 __device__ __forceinline__ void store_components(uint4* H, int s, uint4 e) {
@@ -572,7 +590,7 @@ struct GroupSmem {
     int G;
     int total;
     int glob;        // 0 shared-memory group, 1 global histogram, 2 bin-range passes
-    int safe_floor;  // |dt / P| < 2^50 over the group: floor via floor_magic
+    int safe_floor;  // fold_safe over the group: the fast fold form is exact
     // bin-range passes (one period whose bins exceed shared memory)
     uint4 pad_save[16];  // raw entries of bins 1..oversample (the V42 padding source)
     longlong2 carry;     // exact sums of every bin below the next pass
@@ -582,75 +600,100 @@ struct GroupSmem {
 };
 constexpr int kMpPadMax = 16;  // oversample limit of the bin-range passes
 
-// Histogram slots of one thread's kR points for one period, returned as
-// t = slot - 1.
+// The fast fold form is exact when |d*IP| < 2^50 for every point (floor by
+// magic additions) and, with astropy bins, the phase ph = fma(-P, floor(d*IP), d)
+// -- negative by at most P*|d*IP|*2^-52 where d*IP rounded up past an
+// integer -- stays above -bin_dur, so that int(ph*inv_bin_dur) >= 0 and the
+// guard slot only ever holds points of slot 1: |d*IP| * max(1, P*inv_bin_dur)
+// < 2^40 bounds that error by 2^-12 bins.  dtmax_ip = max |d| / min P,
+// p_ibd = max P * inv_bin_dur.
+template <int GEOM>
+__device__ __forceinline__ bool fold_safe(double dtmax_ip, double p_ibd) {
+    if (!(dtmax_ip < 1.0e15)) return false;
+    return GEOM != ATB_GEOM_BINNED || dtmax_ip * fmax(1.0, p_ibd) < 1099511627776.0;  // 2^40
+}
+
+// Histogram slots of one thread's kR points for one period.
 //   astropy-binned (vbls_v42_parity.cu:65-70): ph = fma(-P, floor(d*IP), d),
-//     slot = min(int(ph*inv_bin_dur) + 1, n_bins), i.e. t = min(max(int, 0), n_bins - 1)
+//     slot = min(int(ph*inv_bin_dur) + 1, n_bins).  int(x) of x in (-1, 0) is 0
+//     (slot 1); the magic addition gives 0 there.  GUARD: that 0 is kept --
+//     slot 0 is a guard entry that finalize_period adds into slot 1 -- and one
+//     unsigned minimum bounds every other value, non-finite inputs (flagged
+//     by the staging) included, by n_bins.  Without GUARD, slot 0 becomes 1.
 //   fixed bins (bls.cu:52-62): ph = d*IP - floor(d*IP) in [0, 1), b = int(ph*n_bins)
 //     in [0, n_bins]; slot = b + 1, where b = n_bins (a product rounded up to
 //     n_bins) is the trash slot n_bins + 1 that no window reads.  The unsigned
-//     minimum keeps non-finite inputs (flagged by the staging) in the trash slot.
-// floor and trunc are computed with exact
-// magic-constant additions, and when the points are time-ordered and the first
-// and last share the cycle index k = floor(d*IP), every point between them has
-// the same k (rounded multiplication and floor are monotone), so k is reused.
-template <int GEOM>
-__device__ __forceinline__ void fold_slots(const double (&d)[kR], bool sorted, bool safe_floor,
-                                           double P, double IP, double ibd, int NB, int (&t)[kR]) {
-    double k0, k7;
-    const double m0 = d[0] * IP, m7 = d[kR - 1] * IP;
-    if (safe_floor) {
-        k0 = floor_magic(m0);
-        k7 = floor_magic(m7);
-    } else {
-        k0 = floor(m0);
-        k7 = floor(m7);
-    }
+//     minimum keeps non-finite inputs inside the period's entries.
+// `safe` (see fold_safe) selects the fast form: floor by exact
+// magic-constant additions, the guard slot, and, when the points are
+// time-ordered and the first and last share the cycle index k = floor(d*IP),
+// one k for all of them (rounded multiplication and floor are monotone).
+// Without `safe`, every point takes floor() and the clamp to [1, n_bins].
+template <int GEOM, bool GUARD>
+__device__ __forceinline__ void fold_slots(const double (&d)[kR], bool sorted, bool safe, double P,
+                                           double IP, double ibd, int NB, unsigned (&e)[kR]) {
     const double nbd = (double)NB;
-    if (sorted && k0 == k7) {
+    if (!safe) {
+#pragma unroll
+        for (int j = 0; j < kR; ++j) {
+            const double m = d[j] * IP;
+            const double k = floor(m);
+            if (GEOM == ATB_GEOM_BINNED) {
+                const int s1 = trunc1_magic(fma(-P, k, d[j]) * ibd);
+                e[j] = (unsigned)min(max(s1, 1), NB);
+            } else {
+                e[j] = min((unsigned)trunc1_magic((m - k) * nbd), (unsigned)NB + 1u);
+            }
+        }
+        return;
+    }
+    // sorted: m0 <= m7, so floor(m7) == k0 exactly when m7 < k0 + 1
+    const double m0 = d[0] * IP, m7 = d[kR - 1] * IP;
+    const double k0 = floor_magic(m0);
+    if (sorted && m7 < k0 + 1.0) {
 #pragma unroll
         for (int j = 0; j < kR; ++j) {
             if (GEOM == ATB_GEOM_BINNED) {
-                const double ph = fma(-P, k0, d[j]);
-                t[j] = min(max(trunc_magic(ph * ibd), 0), NB - 1);
+                const int s1 = trunc1_magic(fma(-P, k0, d[j]) * ibd);
+                e[j] = GUARD ? min((unsigned)s1, (unsigned)NB) : (unsigned)min(max(s1, 1), NB);
             } else {
                 const double m = (j == 0) ? m0 : (j == kR - 1 ? m7 : d[j] * IP);
-                t[j] = (int)min((unsigned)trunc_magic((m - k0) * nbd), (unsigned)NB);
+                e[j] = min((unsigned)trunc1_magic((m - k0) * nbd), (unsigned)NB + 1u);
             }
         }
     } else {
 #pragma unroll
         for (int j = 0; j < kR; ++j) {
             const double m = d[j] * IP;
-            const double k = safe_floor ? floor_magic(m) : floor(m);
+            const double k = floor_magic(m);
             if (GEOM == ATB_GEOM_BINNED) {
-                const double ph = fma(-P, k, d[j]);
-                t[j] = min(max(trunc_magic(ph * ibd), 0), NB - 1);
+                const int s1 = trunc1_magic(fma(-P, k, d[j]) * ibd);
+                e[j] = GUARD ? min((unsigned)s1, (unsigned)NB) : (unsigned)min(max(s1, 1), NB);
             } else {
-                t[j] = (int)min((unsigned)trunc_magic((m - k) * nbd), (unsigned)NB);
+                e[j] = min((unsigned)trunc1_magic((m - k) * nbd), (unsigned)NB + 1u);
             }
         }
     }
 }
 
-// Add one point's words to histogram slot 1 + t (component c of the entry
-// lives at word c ^ rot(1 + t)); `base1` is the shared-memory address of slot 1
-// (H1 the pointer to it for global histograms).  MODE selects the layout
+// Add one point's words to histogram entry e (component c of the entry lives
+// at word c ^ rot(e)); `base0` is the shared-memory address of entry 0 (H0
+// the pointer to it for global histograms).  MODE selects the layout
 // (kPack*); words a..d are the point's components x, y, z, w (unused ones are
 // ignored).
 template <bool GLOB, int MODE>
-__device__ __forceinline__ void hist_add_point(unsigned base1, uint4* H1, int t, unsigned a,
+__device__ __forceinline__ void hist_add_point(unsigned base0, uint4* H0, unsigned e, unsigned a,
                                                unsigned b, unsigned c, unsigned d) {
     if (GLOB) {
-        const unsigned r = ((unsigned)t >> 3) & 3u;
-        unsigned* e = reinterpret_cast<unsigned*>(H1 + t);
-        atomicAdd(e + (0u ^ r), a);
-        if (MODE == kPackSplit) atomicAdd(e + (1u ^ r), b);
-        atomicAdd(e + (2u ^ r), c);
-        if (MODE != kPackTight) atomicAdd(e + (3u ^ r), d);
+        const unsigned r = (e >> 3) & 3u;
+        unsigned* w = reinterpret_cast<unsigned*>(H0 + e);
+        atomicAdd(w + (0u ^ r), a);
+        if (MODE == kPackSplit) atomicAdd(w + (1u ^ r), b);
+        atomicAdd(w + (2u ^ r), c);
+        if (MODE != kPackTight) atomicAdd(w + (3u ^ r), d);
     } else {
-        // base1 + 16 t has four low zero bits; rot(1 + t) << 2 = (t >> 1) & 12
-        const unsigned ad = (base1 + 16u * (unsigned)t) | (((unsigned)t >> 1) & 12u);
+        // base0 + 16 e has four low zero bits; rot(e) << 2 = (e >> 1) & 12
+        const unsigned ad = (base0 + 16u * e) | ((e >> 1) & 12u);
         red_shared_u32(ad, a);
         if (MODE == kPackSplit) red_shared_u32(ad ^ 4u, b);
         red_shared_u32(ad ^ 8u, c);
@@ -694,17 +737,18 @@ __device__ void fold_group(const SearchArgs& a, const GroupSmem& gs, uint4* H, l
         bool sorted = true;
 #pragma unroll
         for (int j = 0; j + 1 < kR; ++j) sorted = sorted && (d[j] <= d[j + 1]);
-        // each point's histogram words (padding points have q_w = q_y = 0)
+        // each point's histogram words (padding points have q_w = q_y = 0);
+        // the stage kernel has already packed the tight words and the count
         unsigned wa[kR], wb[kR], wc[kR], wd[kR];
 #pragma unroll
         for (int j = 0; j < kR; ++j) {
             if (MODE == kPackTight) {
-                wa[j] = (qw[j] != 0 ? (1u << st.cshift) : 0u) + ((unsigned)qy[j] & lomask);
+                wa[j] = (unsigned)qw[j];
                 wb[j] = 0u;
-                wc[j] = (unsigned)(qy[j] >> L);
+                wc[j] = (unsigned)qy[j];
                 wd[j] = 0u;
             } else {
-                wa[j] = MODE == kPackCount ? (qw[j] != 0 ? 1u : 0u) : ((unsigned)qw[j] & lomask);
+                wa[j] = MODE == kPackCount ? (unsigned)qw[j] : ((unsigned)qw[j] & lomask);
                 wb[j] = MODE == kPackCount ? 0u : (unsigned)(qw[j] >> L);
                 wc[j] = (unsigned)qy[j] & lomask;
                 wd[j] = (unsigned)(qy[j] >> L);
@@ -713,18 +757,18 @@ __device__ void fold_group(const SearchArgs& a, const GroupSmem& gs, uint4* H, l
         for (int g = 0; g < G; ++g) {
             const double2 pip = gs.PIP[g];
             const int2 nbb = gs.NBB[g];
-            int t[kR];
-            fold_slots<GEOM>(d, sorted, safe, pip.x, pip.y, st.inv_bin_dur, nbb.x, t);
-            uint4* H1 = H + nbb.y + 1;
-            const unsigned base1 = GLOB ? 0u : (unsigned)__cvta_generic_to_shared(H1);
+            unsigned e[kR];
+            fold_slots<GEOM, GEOM == ATB_GEOM_BINNED && !WIN>(d, sorted, safe, pip.x, pip.y,
+                                                             st.inv_bin_dur, nbb.x, e);
+            uint4* H0 = H + nbb.y;
+            const unsigned base0 = GLOB ? 0u : (unsigned)__cvta_generic_to_shared(H0);
 #pragma unroll
             for (int j = 0; j < kR; ++j) {
                 if (WIN) {
-                    const int tt = t[j] - lo;  // entry tt + 1 of the pass
-                    if ((unsigned)(tt + 1) < W)
-                        hist_add_point<GLOB, MODE>(base1, H1, tt, wa[j], wb[j], wc[j], wd[j]);
+                    const unsigned ee = e[j] - (unsigned)lo;  // entry of the pass
+                    if (ee < W) hist_add_point<GLOB, MODE>(base0, H0, ee, wa[j], wb[j], wc[j], wd[j]);
                 } else {
-                    hist_add_point<GLOB, MODE>(base1, H1, t[j], wa[j], wb[j], wc[j], wd[j]);
+                    hist_add_point<GLOB, MODE>(base0, H0, e[j], wa[j], wb[j], wc[j], wd[j]);
                 }
             }
         }
@@ -758,7 +802,7 @@ __device__ void window_stats(double dw, double dy, double wtot, double ytot, int
 
 // Exact sums (W, Y) of raw histogram entry i in layout MODE: the words the
 // layout uses are read directly (component c of entry i is word c ^ rot(i),
-// at byte offset 4c ^ (((i - 1) >> 1) & 12) in the entry).
+// at byte offset 4c ^ ((i >> 1) & 12) in the entry).
 template <int MODE>
 __device__ __forceinline__ void entry_sums_m(const longlong2* E, int i, const CurveStat& st,
                                              long long& w, long long& y) {
@@ -1146,11 +1190,24 @@ __device__ void finalize_period(const SearchArgs& a, GroupSmem& gs, const Team& 
         // padding copy, vbls_v42_parity.cu:78-80: bins 1..os onto NB-os..NB-1
         // with sequential semantics; when the two ranges are disjoint
         // (NB > 2 os) the copies are independent and run in parallel
+        // first the fold's guard slot 0 (points with int(ph*inv_bin_dur) = 0
+        // from ph*inv_bin_dur in (-1, 0)) joins slot 1; the words are 32-bit
+        // sums, so the entries add word by word
         const int os = a.oversample;
         uint4* R = reinterpret_cast<uint4*>(E);
         if (NB > 2 * os) {
-            if (tm.tid < os) store_components(R, NB - os + tm.tid, load_components(R, 1 + tm.tid));
+            if (tm.tid < os) {
+                uint4 v = load_components(R, 1 + tm.tid);
+                if (tm.tid == 0) {
+                    v = add_words(v, load_components(R, 0));
+                    R[0] = make_uint4(0u, 0u, 0u, 0u);
+                    store_components(R, 1, v);
+                }
+                store_components(R, NB - os + tm.tid, v);
+            }
         } else if (tm.tid == 0) {
+            store_components(R, 1, add_words(load_components(R, 1), load_components(R, 0)));
+            R[0] = make_uint4(0u, 0u, 0u, 0u);
             for (int j = 1, ind = NB - os; j <= os; ++j, ++ind)
                 store_components(R, ind, load_components(R, j));
         }
@@ -1412,7 +1469,8 @@ __device__ void run_group(const SearchArgs& a, GroupSmem& gs, longlong2* H, cons
         fold_group<GEOM, GLOB, kPackSplit>(a, gs, HU, so, n_pad, st);
     __syncthreads();
     const int G = gs.G;
-    // teams of tw warps; multi-warp teams synchronise on named barriers 1..15,
+    // teams of tw warps (a power of two; teams as wide as 1/G of the CTA
+    // measured slower); multi-warp teams synchronise on named barriers 1..15,
     // so at most 15 of them may exist
     int tw = 1;
     while (tw * 2 * G <= kWarps) tw *= 2;
@@ -1484,7 +1542,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) search_kernel(const Search
             if (threadIdx.x == 0) {
                 int g = 0, base = 0;
                 long long p = pn;
-                double ipmax = 0.0;
+                double ipmax = 0.0, pmax = 0.0;
                 while (p < pe && g < kMaxG) {
                     const int li = (int)(p - gs.pb);
                     const double P = gs.tP[li];
@@ -1493,6 +1551,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) search_kernel(const Search
                     if (g > 0 && base + need > a.cap) break;
                     const double IP = 1.0 / P;
                     ipmax = max(ipmax, IP);
+                    pmax = max(pmax, P);
                     gs.PIP[g] = make_double2(P, IP);
                     gs.NBB[g] = make_int2(NB, base);
                     gs.slot[g] = obeg + p;
@@ -1510,7 +1569,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) search_kernel(const Search
                     // a pass must hold the windows of at least 64 starts
                     if (a.cap - 2 - lmax >= 64) gs.glob = 2;
                 }
-                gs.safe_floor = (st.dt_absmax * ipmax < 1.0e15) ? 1 : 0;
+                gs.safe_floor =
+                    fold_safe<GEOM>(st.dt_absmax * ipmax, pmax * st.inv_bin_dur) ? 1 : 0;
             }
             __syncthreads();
             if (gs.glob == 2) {
@@ -1673,12 +1733,12 @@ __global__ void debug_fold_kernel(const double* sdt, long long n, const CurveSta
 #pragma unroll
         for (int j = 0; j + 1 < kR; ++j) sorted = sorted && (d[j] <= d[j + 1]);
         const double IP = 1.0 / P;
-        const bool safe = st.dt_absmax * IP < 1.0e15;
-        int t[kR];
-        fold_slots<GEOM>(d, sorted, safe, P, IP, st.inv_bin_dur, NB, t);
+        const bool safe = fold_safe<GEOM>(st.dt_absmax * IP, P * st.inv_bin_dur);
+        unsigned e[kR];
+        fold_slots<GEOM, GEOM == ATB_GEOM_BINNED>(d, sorted, safe, P, IP, st.inv_bin_dur, NB, e);
 #pragma unroll
-        for (int j = 0; j < kR; ++j)
-            if (ch * kR + j < n) out[p * n + ch * kR + j] = t[j] + 1;
+        for (int j = 0; j < kR; ++j)  // the guard slot 0 is counted in slot 1
+            if (ch * kR + j < n) out[p * n + ch * kR + j] = max((int)e[j], 1);
     }
 }
 

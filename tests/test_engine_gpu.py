@@ -85,6 +85,31 @@ def test_fold_slots_bit_exact(engine):
     assert np.array_equal(slots, ora_slots)
 
 
+def test_binned_negative_phase_points_join_slot_1(engine):
+    """Points whose rounded d*(1/P) reaches an integer that the exact d/P stays
+    below get a phase just under 0, and int(ph/bin_dur) = 0 puts them in V42
+    slot 1: the fold counts them in a guard entry that joins slot 1."""
+    from fractions import Fraction
+    n = 3000
+    t = np.arange(n) * 0.1
+    rng = np.random.default_rng(4)
+    y = R.inject_box(t, 1.0 + rng.normal(0, 1e-3, n), 1.1, 0.35, 0.2, 3e-3).astype(np.float32)
+    periods = np.array([0.3, 1.1, 0.1 * 7, 1.3, 0.9, 2.3])
+    durs = np.array([0.05, 0.1, 0.2])
+    d = t - t[0]
+    neg = sum(1 for P in periods for k, di in zip(np.floor(d * (1.0 / P)), d)
+              if Fraction(float(di)) < Fraction(float(P)) * Fraction(float(k)))
+    assert neg > 100  # the case is present
+    dev = engine.device
+    slots = engine.debug_fold(torch.tensor(t, device=dev), torch.tensor(y, device=dev), None,
+                              torch.tensor(periods, device=dev), torch.tensor(durs, device=dev),
+                              cfg_binned()).cpu().numpy()
+    assert np.array_equal(slots, O.eng_binned(t, y, None, periods, durs, point_bins=True)["point_bins"])
+    for objective in ("snr", "likelihood"):
+        g = run(engine, t, y, None, periods, durs, cfg_binned(objective))
+        assert_bit_exact(g, O.eng_binned(t, y, None, periods, durs, objective=objective), objective)
+
+
 @pytest.mark.parametrize("objective", ["snr", "likelihood"])
 def test_binned_bit_exact_reference_recipe(engine, objective):
     t, y, dy, periods, durs = R.v42_test_recipe()
