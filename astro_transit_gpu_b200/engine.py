@@ -573,6 +573,14 @@ class BatchSession:
         else:
             self.plan.execute(s)
 
+    def close(self) -> None:
+        """Release the graphs, the plan and the device and pinned buffers
+        (after the work enqueued so far has finished)."""
+        torch.cuda.synchronize(self.batch.device)
+        self.step_graph = self.search_graph = None
+        self.plan.close()
+        self.dev_in, self.outputs, self.host, self.host_out = {}, {}, {}, {}
+
 
 def _grid_arrays(g, nc):
     if is_shared_grid(g):

@@ -26,6 +26,7 @@ host cores (this workload's CPU path) on rank 0.
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import subprocess
@@ -328,8 +329,11 @@ def run_serving(args, device):
                          durations=R.C2_DURATIONS[:4 + int(rng.integers(0, 5))], method="fast"))
     gaps = rng.exponential(1.0 / args.serving_rate, n_req)
     with BLSServer(device=device, memory_budget=120e9, max_batch=512, n_streams=2) as srv:
-        # warm-up request (library load, allocator pools)
+        # warm-up (library load, allocator pools at the sizes of large
+        # batches): one request, then a burst of 64 at once; not timed
         srv.submit(**reqs[0]).result(timeout=300)
+        for f in [srv.submit(**r) for r in reqs[:64]]:
+            f.result(timeout=300)
         srv._latencies.clear()
         srv._t_first = srv._t_last = None
         srv._batches = 0
@@ -480,6 +484,11 @@ def main():
                                 "sample": sample,
                                 "max_rel_power_err_vs_gpu": rel}
     if world == 1 and not args.no_serving:
+        # the server runs alone on the device, as in a serving process
+        sess.close()
+        del sess, plan
+        gc.collect()
+        torch.cuda.empty_cache()
         line["serving"] = run_serving(args, dev)
     if rank == 0:
         print(json.dumps(line), flush=True)
