@@ -110,6 +110,31 @@ def test_binned_negative_phase_points_join_slot_1(engine):
         assert_bit_exact(g, O.eng_binned(t, y, None, periods, durs, objective=objective), objective)
 
 
+def test_fold_outside_the_fast_form_range(engine):
+    """Time spans so long that |d/P| * P/bin_dur reaches 2^40 (astropy bins)
+    or |d/P| reaches 1e15 (fixed bins): the fold takes floor() and the full
+    clamp per point, still bit-exact against the oracle."""
+    rng = np.random.default_rng(12)
+    n = 2000
+    dev = engine.device
+    for t_span, periods, cfg, ora in (
+            (2e10, np.array([0.9, 1.3, 2.0]), cfg_binned(), O.eng_binned),
+            (3e15, np.array([1.1, 1.7, 2.9]), cfg_fixed(64), O.eng_fixed)):
+        t = np.sort(rng.uniform(0.0, t_span, n))
+        y = (1.0 + rng.normal(0, 1e-3, n)).astype(np.float32)
+        durs = np.array([0.1, 0.2])
+        slots = engine.debug_fold(torch.tensor(t, device=dev), torch.tensor(y, device=dev), None,
+                                  torch.tensor(periods, device=dev), torch.tensor(durs, device=dev),
+                                  cfg).cpu().numpy()
+        kw = {} if ora is O.eng_binned else {"n_bins": 64}
+        want = ora(t, y, None, periods, durs, point_bins=True, **kw)["point_bins"]
+        if ora is O.eng_fixed:
+            want = np.where(want < 0, 65, want)
+        assert np.array_equal(slots, want)
+        g = run(engine, t, y, None, periods, durs, cfg)
+        assert_bit_exact(g, ora(t, y, None, periods, durs, **kw))
+
+
 @pytest.mark.parametrize("objective", ["snr", "likelihood"])
 def test_binned_bit_exact_reference_recipe(engine, objective):
     t, y, dy, periods, durs = R.v42_test_recipe()
