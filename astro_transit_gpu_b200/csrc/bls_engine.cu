@@ -64,6 +64,7 @@ constexpr int kMaxG = 64;              // periods per shared-memory group
 constexpr int kMaxDur = 32;            // durations per curve
 constexpr int kStageAlign = 32;        // staged curves start at multiples of 32 points
 constexpr int kStageBlock = 256;
+constexpr int kChunk = 32 * kR;        // staged points of one warp's fold step
 constexpr double kMagicSlot = 4503599627370497.0;   // 2^52 + 1: x + C (rz) = 2^52 + int(x) + 1, x in (-1, 2^31 - 1)
 constexpr double kMagicFloor = 6755399441055744.0;  // 1.5*2^52: (m + C)(rd) - C = floor(m), |m| < 2^50
 
@@ -118,6 +119,7 @@ struct CurveStat {
     int cnt_win;    // uniform weights and fewer than 2^24 points: the window search
                     // works on exact FP32 point counts instead of FP64 weight sums
     int n_cnt;      // number of points (cnt_win)
+    int ilv;        // staged order interleaved within whole chunks (staged_pos)
 };
 
 struct StageArgs {
@@ -198,6 +200,25 @@ __device__ __forceinline__ int q_scale(double m, int qbits) {
 __device__ __forceinline__ int bitlen64(long long n) { return n <= 0 ? 0 : 64 - __clzll(n); }
 __device__ __forceinline__ int curve_lobits(long long n) { return min(30, 32 - bitlen64(n)); }
 __device__ __forceinline__ int curve_qbits(long long n) { return min(26, 63 - 2 * bitlen64(n)); }
+
+// Staged order of a curve's points.  Interleaved (n_full > 0): in every
+// whole chunk of kChunk points the kR staged values of lane l are points l,
+// l + 32, l + 64, ... of the chunk, so that the lanes of a warp fold 32
+// consecutive points at a time, while each thread's values stay
+// time-ordered; points of the last, partial chunk keep their order.  n_full =
+// the points in whole chunks, 0 for the plain order.
+__device__ __forceinline__ long long staged_pos(long long i, long long n_full) {
+    if (i >= n_full) return i;
+    const int r = (int)(i % kChunk);
+    return i - r + (r & 31) * kR + (r >> 5);
+}
+
+// the inverse: the point held at staged position q
+__device__ __forceinline__ long long staged_point(long long q, long long n_full) {
+    if (q >= n_full) return q;
+    const int r = (int)(q % kChunk);
+    return q - r + (r % kR) * 32 + r / kR;
+}
 
 // floor(m) for |m| < 2^50 with two full-rate FP64 additions (exact)
 __device__ __forceinline__ double floor_magic(double m) {
@@ -436,6 +457,23 @@ __global__ void __launch_bounds__(kStageBlock) stage_kernel(const StageArgs a) {
     //   split  q_w and q_y as they are
     const int lob = packmode == kPackTight ? 32 - 2 * tight_bits : curve_lobits(n);
     const int csh = 32 - tight_bits;
+    // Staged order: with astropy bins (one bin width for every period),
+    // interleaved when the mean spacing of the points reaches the bin width
+    // -- a warp's 32 consecutive points then fall in distinct bins, while
+    // lanes kR points apart would fall kR bins apart and share banks.  Denser
+    // curves keep the plain order: interleaved, up to 32 lanes would add to
+    // the same few bins, which serialises.  Fixed bins (P / n_bins, mostly
+    // far wider) keep it too; interleaved, an uneven batch of the fast
+    // method measured 14 % slower.
+    double width = 0.0;
+    if (a.geometry == ATB_GEOM_BINNED) {
+        const double* dur = a.durations + a.dur_beg[c];
+        double md = dur[0];
+        for (int k = 1; k < a.dur_cnt[c]; ++k) md = min(md, dur[k]);
+        width = md / (double)a.oversample;
+    }
+    const bool ilv = n > 1 && width > 0.0 && tmax >= width * (double)(n - 1);
+    const long long n_full = ilv ? n_pad / kChunk * kChunk : 0;
     long long qw_tot = 0, qy_tot = 0, qy_abs = 0;
     for (long long i = threadIdx.x; i < n_pad; i += kStageBlock) {
         double d = 0.0;
@@ -453,9 +491,10 @@ __global__ void __launch_bounds__(kStageBlock) stage_kernel(const StageArgs a) {
         } else if (packmode == kPackCount) {
             sa = qa != 0 ? 1 : 0;
         }
-        a.sdt[so + i] = d;
-        a.sqw[so + i] = sa;
-        a.sqy[so + i] = sb;
+        const long long q = so + staged_pos(i, n_full);
+        a.sdt[q] = d;
+        a.sqw[q] = sa;
+        a.sqy[q] = sb;
         qw_tot += qa;
         qy_tot += qb;
         qy_abs += qb < 0 ? -(long long)qb : (long long)qb;
@@ -505,6 +544,7 @@ __global__ void __launch_bounds__(kStageBlock) stage_kernel(const StageArgs a) {
         st.occ_bits = tight_bits;
         st.cnt_win = (uniform && n < (1LL << 24)) ? 1 : 0;
         st.n_cnt = st.cnt_win ? (int)n : 0;
+        st.ilv = ilv ? 1 : 0;
         a.stats[c] = st;
     }
 }
@@ -1719,6 +1759,7 @@ __global__ void debug_fold_kernel(const double* sdt, long long n, const CurveSta
     const long long n_pad = (n + kR - 1) / kR * kR;
     const long long chunks = n_pad / kR;
     const CurveStat st = stats[0];
+    const long long n_full = st.ilv ? n_pad / kChunk * kChunk : 0;
     for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < chunks * n_periods;
          idx += (long long)gridDim.x * blockDim.x) {
         const long long p = idx / chunks, ch = idx % chunks;
@@ -1737,8 +1778,10 @@ __global__ void debug_fold_kernel(const double* sdt, long long n, const CurveSta
         unsigned e[kR];
         fold_slots<GEOM, GEOM == ATB_GEOM_BINNED>(d, sorted, safe, P, IP, st.inv_bin_dur, NB, e);
 #pragma unroll
-        for (int j = 0; j < kR; ++j)  // the guard slot 0 is counted in slot 1
-            if (ch * kR + j < n) out[p * n + ch * kR + j] = max((int)e[j], 1);
+        for (int j = 0; j < kR; ++j) {  // the guard slot 0 is counted in slot 1
+            const long long i = staged_point(ch * kR + j, n_full);
+            if (i < n) out[p * n + i] = max((int)e[j], 1);
+        }
     }
 }
 
