@@ -582,6 +582,88 @@ class BatchSession:
         self.dev_in, self.outputs, self.host, self.host_out = {}, {}, {}, {}
 
 
+class PipelinedSession:
+    """A fixed-shape batch split into ``parts`` runs of consecutive curves,
+    each a :class:`BatchSession` with its own stream.  A step forks from the
+    caller's stream, runs every part (inputs in, search, outputs back) on its
+    own stream and joins again, so one part's copies cross PCIe while another
+    part searches, and one search's last tiles overlap the next one's first.
+    Each curve's result depends only on that curve, so the results are those
+    of one session over the whole batch."""
+
+    def __init__(self, engine: BLSEngine, point_offset: np.ndarray, periods, durations,
+                 config: SearchConfig, parts: int = 4, y_dtype=np.float32,
+                 weighted: bool = True, fields: Sequence[str] = OUTPUT_FIELDS):
+        pt = _i64(point_offset)
+        nc = len(pt) - 1
+        if nc < 1:
+            raise ValueError("a pipelined session needs at least one curve")
+        parts = max(1, min(int(parts), nc))
+        self.bounds = [int(round(i * nc / parts)) for i in range(parts + 1)]
+        self.point_offset = pt
+        self.device = engine.device
+        self.sessions: List[BatchSession] = []
+        self.streams = [torch.cuda.Stream(engine.device) for _ in range(parts)]
+        for a, b in zip(self.bounds[:-1], self.bounds[1:]):
+            per = periods if is_shared_grid(periods) else list(periods[a:b])
+            dur = durations if is_shared_grid(durations) else list(durations[a:b])
+            self.sessions.append(BatchSession(engine, pt[a:b + 1] - pt[a], per, dur, config,
+                                              y_dtype, weighted, fields))
+
+    @property
+    def h2d_bytes(self) -> int:
+        return sum(s.h2d_bytes for s in self.sessions)
+
+    @property
+    def d2h_bytes(self) -> int:
+        return sum(s.d2h_bytes for s in self.sessions)
+
+    @property
+    def kernel_count(self) -> int:
+        return sum(s.plan.kernel_count for s in self.sessions)
+
+    def load(self, t: np.ndarray, y: np.ndarray, w: Optional[np.ndarray] = None) -> None:
+        """Fill every part's pinned host input buffers (flattened curves)."""
+        t, y = np.ravel(t), np.ravel(y)
+        w = None if w is None else np.ravel(w)
+        for s, a, b in zip(self.sessions, self.bounds[:-1], self.bounds[1:]):
+            lo, hi = int(self.point_offset[a]), int(self.point_offset[b])
+            s.load(t[lo:hi], y[lo:hi], None if w is None else w[lo:hi])
+
+    def capture(self) -> None:
+        for s in self.sessions:
+            s.capture()
+
+    def _each(self, stream: Optional[torch.cuda.Stream], fn) -> None:
+        main = stream if stream is not None else torch.cuda.current_stream(self.device)
+        fork = torch.cuda.Event()
+        fork.record(main)
+        for s, st in zip(self.sessions, self.streams):
+            st.wait_event(fork)
+            fn(s, st)
+            done = torch.cuda.Event()
+            done.record(st)
+            main.wait_event(done)
+
+    def run(self, stream: Optional[torch.cuda.Stream] = None) -> List[Dict[str, torch.Tensor]]:
+        """Enqueue one step; `stream` (default: the current stream) waits for
+        every part, after which each part's pinned host outputs are valid."""
+        self._each(stream, lambda s, st: s.run(st))
+        return [s.host_out for s in self.sessions]
+
+    def search(self, stream: Optional[torch.cuda.Stream] = None) -> None:
+        """The searches alone on the resident inputs, joined on `stream`."""
+        self._each(stream, lambda s, st: s.search(st))
+
+    def check(self) -> None:
+        for s in self.sessions:
+            s.plan.check()
+
+    def close(self) -> None:
+        for s in self.sessions:
+            s.close()
+
+
 def _grid_arrays(g, nc):
     if is_shared_grid(g):
         arr = np.atleast_1d(np.asarray(g, np.float64))

@@ -427,6 +427,38 @@ def test_batch_session_graph_replay_matches_eager(engine):
         assert torch.equal(graphed.host_out[k], eager.host_out[k]), k
 
 
+@pytest.mark.parametrize("graphs", [False, True])
+def test_pipelined_session_equals_one_session(engine, graphs):
+    """A ragged batch (own period grid per curve) split into runs of curves on
+    their own streams gives, bit for bit, one session's outputs."""
+    from astro_transit_gpu_b200.engine import BatchSession, PipelinedSession, SearchConfig
+    cs = R.mixed_batch(n_curves=7, seed=31, max_points=4000)
+    t, y, dy, per = zip(*cs)
+    w = [(1 / d.astype(np.float64) ** 2).astype(np.float32) for d in dy]
+    pt = np.zeros(8, np.int64)
+    np.cumsum([len(a) for a in t], out=pt[1:])
+    per = [p[:: max(1, len(p) // 700)] for p in per]
+    durs = list(R.C2_DURATIONS)
+    cfg = SearchConfig("parity", objective="likelihood")
+    one = BatchSession(engine, pt, per, durs, cfg)
+    one.load(np.concatenate(t), np.concatenate(y), np.concatenate(w))
+    one.run()
+    torch.cuda.synchronize()
+    one.plan.check()
+    ps = PipelinedSession(engine, pt, per, durs, cfg, parts=3)
+    ps.load(np.concatenate(t), np.concatenate(y), np.concatenate(w))
+    if graphs:
+        ps.capture()
+    outs = ps.run()
+    torch.cuda.synchronize()
+    ps.check()
+    assert ps.bounds == [0, 2, 5, 7]
+    for k, v in one.host_out.items():
+        assert torch.equal(torch.cat([o[k] for o in outs]), v), k
+    ps.close()
+    one.close()
+
+
 # ------------------------------------------------------ winner-take-all ---
 
 @pytest.mark.parametrize("method", ["fast", "parity"])
