@@ -167,6 +167,14 @@ class BLSServer:
                 "max_held_bytes": self._max_held,
             }
 
+    def reset_stats(self) -> None:
+        """Forget the latencies and batch count gathered so far (after a
+        warm-up, say)."""
+        with self._cv:
+            self._latencies.clear()
+            self._t_first = self._t_last = None
+            self._batches = 0
+
     def close(self) -> None:
         """Finish every submitted request, then stop the worker."""
         with self._cv:
