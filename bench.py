@@ -479,7 +479,8 @@ def main():
                 "d2h_bytes_per_step": psess.d2h_bytes, "ms_per_step": ms_e2e / args.steps,
                 "api": f"PipelinedSession.run ({E2E_PARTS} runs of curves on {E2E_PARTS} "
                        "streams, each a BatchSession: pinned host buffers, CUDA graph)",
-                "outputs_equal_resident_run": bool(e2e_same)},
+                "outputs_equal_resident_run": bool(e2e_same),
+                "gpu_launches": psess.kernel_count * args.steps},
         "gpu_launches": plan.kernel_count * args.steps,
         "roofline": {
             "bound": "smem",
