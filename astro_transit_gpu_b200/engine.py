@@ -599,7 +599,7 @@ class PipelinedSession:
         if nc < 1:
             raise ValueError("a pipelined session needs at least one curve")
         parts = max(1, min(int(parts), nc))
-        self.bounds = [int(round(i * nc / parts)) for i in range(parts + 1)]
+        self.bounds = [i * nc // parts for i in range(parts + 1)]  # no run is empty
         self.point_offset = pt
         self.device = engine.device
         self.sessions: List[BatchSession] = []

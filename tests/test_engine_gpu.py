@@ -452,7 +452,7 @@ def test_pipelined_session_equals_one_session(engine, graphs):
     outs = ps.run()
     torch.cuda.synchronize()
     ps.check()
-    assert ps.bounds == [0, 2, 5, 7]
+    assert ps.bounds == [0, 2, 4, 7]
     for k, v in one.host_out.items():
         assert torch.equal(torch.cat([o[k] for o in outs]), v), k
     ps.close()
