@@ -85,6 +85,27 @@ def test_fold_slots_bit_exact(engine):
     assert np.array_equal(slots, ora_slots)
 
 
+def test_fold_slots_bit_exact_precision_sample(engine):
+    """1e7 per-point bin indices of a precision-stress curve (200 000 points
+    over 13 sectors, t offset > 1300 d) at 50 periods spread over its
+    0.5-150 d grid, including the bin-range-pass periods, against the FP64
+    fold; then every output of those periods bit-exact."""
+    rng = np.random.default_rng(77)
+    t, y, dy, _ = R.precision_curve(rng)
+    w = (1 / dy.astype(np.float64) ** 2).astype(np.float32)
+    periods = R.precision_periods()[::2000]
+    durs = R.C3_DURATIONS
+    dev = engine.device
+    slots = engine.debug_fold(torch.tensor(t, device=dev), torch.tensor(y, device=dev),
+                              torch.tensor(w, device=dev), torch.tensor(periods, device=dev),
+                              torch.tensor(durs, device=dev), cfg_binned()).cpu().numpy()
+    assert slots.size == 50 * 200_000
+    ora = O.eng_binned(t, y, w, periods, durs, objective="likelihood", point_bins=True)
+    assert np.array_equal(slots, ora["point_bins"])
+    g = run(engine, t, y, w, periods, durs, cfg_binned("likelihood"))
+    assert_bit_exact(g, ora, "precision sample")
+
+
 def test_binned_negative_phase_points_join_slot_1(engine):
     """Points whose rounded d*(1/P) reaches an integer that the exact d/P stays
     below get a phase just under 0, and int(ph/bin_dur) = 0 puts them in V42
