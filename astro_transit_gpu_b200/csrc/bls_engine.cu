@@ -1862,8 +1862,13 @@ struct atb_handle {
     int n_sm = 0;
     int smem_optin = 0;
     int smem_per_sm = 0;
+    // the stream-ordered scratch of asynchronous plans; it keeps up to
+    // kPoolKeepBytes mapped across synchronisations, so that a plan made for
+    // each call of a loop does not map and unmap device memory every time
+    cudaMemPool_t pool = nullptr;
     std::string err;
 };
+constexpr unsigned long long kPoolKeepBytes = 1ull << 30;
 
 struct atb_plan {
     atb_handle* h = nullptr;
@@ -1913,7 +1918,9 @@ template <typename T>
 int plan_alloc(atb_plan* p, T** out, size_t count) {
     void* ptr = nullptr;
     const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
-    cudaError_t e = p->async ? cudaMallocAsync(&ptr, bytes, p->stream) : cudaMalloc(&ptr, bytes);
+    cudaError_t e = !p->async     ? cudaMalloc(&ptr, bytes)
+                    : p->h->pool ? cudaMallocFromPoolAsync(&ptr, bytes, p->h->pool, p->stream)
+                                 : cudaMallocAsync(&ptr, bytes, p->stream);
     if (e != cudaSuccess)
         return fail(p->h, ATB_ENOMEM, "cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(e));
     p->allocs.push_back(ptr);
@@ -1980,11 +1987,26 @@ int atb_create(int device, atb_handle** out) {
     cudaDeviceGetAttribute(&h->n_sm, cudaDevAttrMultiProcessorCount, device);
     cudaDeviceGetAttribute(&h->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
     cudaDeviceGetAttribute(&h->smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device);
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    if (cudaMemPoolCreate(&h->pool, &props) == cudaSuccess) {
+        unsigned long long keep = kPoolKeepBytes;
+        cudaMemPoolSetAttribute(h->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    } else {
+        h->pool = nullptr;  // the device's default pool serves instead
+        cudaGetLastError();
+    }
     *out = h;
     return ATB_OK;
 }
 
-void atb_destroy(atb_handle* h) { delete h; }
+void atb_destroy(atb_handle* h) {
+    // allocations still outstanding keep the pool alive until they are freed
+    if (h && h->pool) cudaMemPoolDestroy(h->pool);
+    delete h;
+}
 
 int atb_last_error(const atb_handle* h, char* buf, size_t len) {
     if (!h) return 0;

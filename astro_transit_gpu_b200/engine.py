@@ -433,10 +433,14 @@ class BLSEngine:
 
     def search(self, batch: CurveBatch, config: SearchConfig,
                stream: Optional[torch.cuda.Stream] = None) -> Dict[str, torch.Tensor]:
-        """Plan, execute, check (synchronises) and return the output tensors."""
-        plan = self.plan(batch, config)
+        """Plan, execute, check (synchronises) and return the output tensors.
+        The plan is made, run and released in `stream`'s order (default: the
+        current stream), so its scratch comes from the engine's stream-ordered
+        pool and no device-wide allocation or release runs per call."""
+        s = stream if stream is not None else torch.cuda.current_stream(batch.device)
+        plan = self.plan(batch, config, stream=s)
         try:
-            plan.execute(stream)
+            plan.execute(s)
             plan.check()
             return plan.outputs
         finally:
