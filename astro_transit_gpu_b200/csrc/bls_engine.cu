@@ -1994,6 +1994,11 @@ int atb_create(int device, atb_handle** out) {
     if (cudaMemPoolCreate(&h->pool, &props) == cudaSuccess) {
         unsigned long long keep = kPoolKeepBytes;
         cudaMemPoolSetAttribute(h->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        // memory freed on one stream goes to another only once that free has
+        // completed: the pool never makes a plan wait for another stream's
+        // batch (a server's small request behind a large one)
+        int no = 0;
+        cudaMemPoolSetAttribute(h->pool, cudaMemPoolReuseAllowInternalDependencies, &no);
     } else {
         h->pool = nullptr;  // the device's default pool serves instead
         cudaGetLastError();
