@@ -602,17 +602,25 @@ class PipelinedSession:
         nc = len(pt) - 1
         if nc < 1:
             raise ValueError("a pipelined session needs at least one curve")
-        parts = max(1, min(int(parts), nc))
-        self.bounds = [i * nc // parts for i in range(parts + 1)]  # no run is empty
+        self.bounds = self.run_bounds(nc, parts)
         self.point_offset = pt
         self.device = engine.device
         self.sessions: List[BatchSession] = []
-        self.streams = [torch.cuda.Stream(engine.device) for _ in range(parts)]
+        self.streams = [torch.cuda.Stream(engine.device) for _ in self.bounds[1:]]
         for a, b in zip(self.bounds[:-1], self.bounds[1:]):
             per = periods if is_shared_grid(periods) else list(periods[a:b])
             dur = durations if is_shared_grid(durations) else list(durations[a:b])
             self.sessions.append(BatchSession(engine, pt[a:b + 1] - pt[a], per, dur, config,
                                               y_dtype, weighted, fields))
+
+    @staticmethod
+    def run_bounds(n_curves: int, parts: int) -> List[int]:
+        """Curve boundaries of min(parts, n_curves) runs of nearly equal
+        size: run i holds curves bounds[i] .. bounds[i+1]-1, none is empty."""
+        if n_curves < 1:
+            raise ValueError("a pipelined session needs at least one curve")
+        parts = max(1, min(int(parts), n_curves))
+        return [i * n_curves // parts for i in range(parts + 1)]
 
     @property
     def h2d_bytes(self) -> int:
