@@ -222,6 +222,35 @@ def test_cap_reproduces_reference_pileup():
     assert (pb[2] == 1999).sum() > (pb[1] == 1999).sum()  # more pile-up at longer period
 
 
+def test_binned_slots_match_exact_restatement_at_cycle_edges():
+    """The oracle's per-point V42 slot, min(int(ph * inv_bin) + 1, n_bins)
+    with ph = fma(-P, floor(d * (1/P)), d) (vbls_v42_parity.cu:65-70), against
+    an independent restatement: the fma rounded once from its exact rational
+    value.  Times on a 0.1 d grid put many points where d*(1/P) rounds onto
+    an integer the exact d/P stays below, so ph is just under 0 and int()
+    gives 0 (slot 1)."""
+    from fractions import Fraction
+    n = 1500
+    t = np.arange(n) * 0.1
+    y = np.ones(n, np.float32)
+    periods = np.array([0.3, 1.1, 0.1 * 7, 0.9])
+    durs = np.array([0.05, 0.1])
+    pb = O.eng_binned(t, y, None, periods, durs, point_bins=True)["point_bins"]
+    d = t - t[0]
+    ibd = 1.0 / (0.05 / 10)
+    negative = 0
+    for p, P in enumerate(periods):
+        nb = math.ceil(P * ibd) + 10
+        ks = np.floor(d * (1.0 / P))
+        for i in range(n):
+            exact = Fraction(float(d[i])) - Fraction(float(P)) * Fraction(float(ks[i]))
+            ph = float(exact)  # round to nearest, as one fma does
+            negative += ph < 0.0
+            slot = min(int(ph * ibd) + 1, nb)
+            assert pb[p, i] == slot, (P, i, ph)
+    assert negative > 50
+
+
 def test_oracle_rejects_bad_arguments():
     t = np.linspace(0, 1, 10)
     with pytest.raises(ValueError):
