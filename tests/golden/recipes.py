@@ -219,3 +219,16 @@ def precision_periods(n=100_000, pmin=0.5, pmax=150.0):
 
 
 C3_DURATIONS = np.geomspace(0.02, 0.3, 8)
+
+
+def mixed_spec_indexed(seed, i):
+    """(n_sectors, cadence, n, n_periods) of curve i of the indexed uneven
+    batch: every curve draws from its own generator, seeded by (seed, i), so a
+    rank can make exactly its share of a large batch."""
+    return mixed_curve_spec(np.random.default_rng([int(seed), int(i)]))
+
+
+def mixed_curve_indexed(seed, i):
+    """Curve i of the indexed uneven batch: (t, y, dy, periods)."""
+    rng = np.random.default_rng([int(seed), int(i)])
+    return mixed_curve(rng, *mixed_curve_spec(rng))
