@@ -32,7 +32,7 @@ EXPORTS = (
     "atb_plan_create", "atb_plan_execute", "atb_plan_check", "atb_plan_kernel_count",
     "atb_plan_scratch_bytes", "atb_plan_destroy", "atb_search", "atb_run_gpu_bls",
     "atb_run_vbls_exact_parity", "atb_debug_fold", "atb_plan_profile",
-    "atb_bench_smem_red_u64", "atb_bench_dfma", "atb_search_curve_static",
+    "atb_bench_smem_red_u64", "atb_bench_smem_red_u32", "atb_bench_dfma", "atb_search_curve_static",
     "atb_plan_curve_layout", "atb_plan_create_async", "atb_plan_top_k",
 )
 
@@ -119,12 +119,13 @@ def load(build_if_missing: bool = True):
         _dp = ctypes.POINTER(ctypes.c_double)
         L.atb_plan_profile.argtypes = [_vp, _vp, _fp, _fp, _fp]
         L.atb_bench_smem_red_u64.argtypes = [_vp, ctypes.c_int, _dp]
+        L.atb_bench_smem_red_u32.argtypes = [_vp, ctypes.c_int, _dp]
         L.atb_bench_dfma.argtypes = [_vp, _dp]
         L.atb_search_curve_static.argtypes = [ctypes.POINTER(Params), _vp, _vp, _i32, _vp, _i64,
                                               _vp, _i64, _vp, _i32, _vp, _vp, _vp, _vp, _vp, _vp,
                                               _vp, _vp, ctypes.c_char_p, ctypes.c_size_t]
         for fn in ("atb_search_curve_static", "atb_plan_profile", "atb_bench_smem_red_u64",
-                   "atb_bench_dfma",
+                   "atb_bench_smem_red_u32", "atb_bench_dfma",
                    "atb_create", "atb_last_error", "atb_plan_create", "atb_plan_create_async",
                    "atb_plan_execute", "atb_plan_top_k",
                    "atb_plan_check", "atb_plan_kernel_count", "atb_search", "atb_run_gpu_bls",

@@ -4,18 +4,19 @@
 // Hot path (one astropy-style BLS per (light curve, period)):
 //   stage kernel   one CTA per curve: t_start = t[0], dt = t - t_start (FP64),
 //                  deterministic fixed-point staging q_w = rint(w*2^s_w),
-//                  q_y = rint(w*(y-c)*2^s_y) (|q| <= 2^26), per-curve totals.
-//   search kernel  persistent; CTAs pop (curve, 64-period) tiles from a device
-//                  counter.  Periods of a tile are packed into groups whose
-//                  histograms fit shared memory; each thread keeps 8
-//                  consecutive points in registers and folds them into every
+//                  q_y = rint(w*(y-c)*2^s_y) (|q| <= 2^26), per-curve totals,
+//                  the curve's histogram word layout (kPack*) and staged order.
+//   search kernel  persistent; CTAs pop (curve, period-chunk) tiles from a
+//                  device counter.  Periods of a tile are packed into groups
+//                  whose histograms fit shared memory; each thread keeps kR = 4
+//                  time-ordered points in registers and folds them into every
 //                  period of the group (FP64 fold, identical to the reference's
-//                  per-point formula), merging runs of equal bins in registers
-//                  before a 64-bit shared-memory reduction.  Teams of warps
-//                  then scan each histogram (exact int64 -> exact FP64),
-//                  evaluate every (start, duration) window in FP32 with an
-//                  exact rational comparison, and re-evaluate the winner in
-//                  FP64.
+//                  per-point formula), adding each point's exact integer sums
+//                  to its bin with two to four 32-bit shared-memory reductions
+//                  on split words.  Teams of warps then scan each histogram
+//                  (exact int64 -> exact FP64), evaluate every (start,
+//                  duration) window in FP32 with an exact rational
+//                  comparison, and re-evaluate the winner in FP64.
 //   best kernel    per-curve argmax over the period grid.
 //
 // Reference semantics followed (paths within ubunbun18/Astro_Transit_GPU):
@@ -29,7 +30,6 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -324,7 +324,8 @@ __device__ long long block_sum_ll(long long v, long long* sh) {
 //   M = (floor(T / P_min) + 3) * K,
 // T = time span, K = most points inside any closed time window of one bin width
 // (astropy-binned: min(duration)/oversample; fixed: P_max/n_bins), widened by a
-// relative 1e-6 for rounding.  Requires time-ordered points.
+// relative 1e-6 for rounding.  Requires time-ordered points and, for
+// astropy bins, a bin cap (max_bins) that no period of the grid reaches.
 __device__ int occupancy_bits(const StageArgs& a, int c, const double* t, long long n, double* shd,
                               long long* shl) {
     // time order
@@ -351,6 +352,12 @@ __device__ int occupancy_bits(const StageArgs& a, int c, const double* t, long l
         double min_dur = dur[0];
         for (int k = 1; k < a.dur_cnt[c]; ++k) min_dur = min(min_dur, dur[k]);
         width = min_dur / (double)a.oversample;
+        // a bin cap that some period reaches piles points into the last bin
+        // (vbls_v42_parity.cu:70): no bound then.  Bin counts grow with the
+        // period, so the largest period decides (same arithmetic as the search).
+        if (a.max_bins > 0 &&
+            binned_nbins(pmax, 1.0 / width, a.oversample, 0) >= a.max_bins)
+            return 64;
     } else {
         width = pmax / (double)a.n_bins_fixed;
     }
@@ -435,8 +442,7 @@ __global__ void __launch_bounds__(kStageBlock) stage_kernel(const StageArgs a) {
     const bool uniform = n > 0 && qw_min == qw_max;
     int packmode = uniform ? kPackCount : kPackSplit;
     int tight_bits = 64;
-    if (uniform && a.periods && !(a.geometry == ATB_GEOM_BINNED && a.max_bins > 0))
-        tight_bits = occupancy_bits(a, c, t, n, shd, shl);
+    if (uniform && a.periods) tight_bits = occupancy_bits(a, c, t, n, shd, shl);
     if (uniform && tight_bits <= kTightMaxBits && qbits <= 26) packmode = kPackTight;
     const int qbits_y = qbits;
     const double shift = sqw != 0 ? ldexp((double)sqa / (double)sqw, s_w - s_a) : 0.0;
@@ -1810,10 +1816,12 @@ __global__ void nbins_max_kernel(int n_curves, const long long* per_beg, const l
 // microbenchmarks for the roofline denominators
 // ----------------------------------------------------------------------------
 
-constexpr int kBenchSlots = 4096;  // 32 KiB of u64 counters
+constexpr int kBenchSlots = 4096;  // counters of the reduction benchmark
 
-// 64-bit shared-memory reductions: pattern 0 = each warp's lanes hit 32
-// consecutive counters (conflict-free), pattern 1 = pseudo-random counters.
+// Shared-memory reductions of 64-bit (WIDE) or 32-bit counters: pattern 0 =
+// each warp's lanes hit 32 consecutive counters (conflict-free), pattern 1 =
+// pseudo-random counters.
+template <bool WIDE>
 __global__ void __launch_bounds__(kBlock) bench_smem_red_kernel(int iters, int pattern,
                                                                 unsigned long long* sink) {
     __shared__ unsigned long long h[kBenchSlots];
@@ -1829,7 +1837,10 @@ __global__ void __launch_bounds__(kBlock) bench_smem_red_kernel(int iters, int p
             x = x * 1664525u + 1013904223u;
             slot = (x >> 9) & (kBenchSlots - 1);
         }
-        asm volatile("red.shared.add.u64 [%0], %1;" ::"r"(base + slot * 8u), "l"(1ULL) : "memory");
+        if (WIDE)
+            asm volatile("red.shared.add.u64 [%0], %1;" ::"r"(base + slot * 8u), "l"(1ULL) : "memory");
+        else
+            asm volatile("red.shared.add.u32 [%0], %1;" ::"r"(base + slot * 4u), "r"(1u) : "memory");
     }
     __syncthreads();
     if (threadIdx.x == 0) atomicAdd(sink, h[blockIdx.x & (kBenchSlots - 1)]);
@@ -1967,6 +1978,31 @@ int launch_stage(atb_plan* p, cudaStream_t s) {
     else
         stage_kernel<float><<<p->n_curves, kStageBlock, 0, s>>>(p->sa);
     ATB_CUDA(p->h, cudaGetLastError());
+    return ATB_OK;
+}
+
+template <bool WIDE>
+int bench_smem_red(atb_handle* h, int pattern, double* reductions_per_s) {
+    if (!h || !reductions_per_s) return ATB_EINVAL;
+    ATB_CUDA(h, cudaSetDevice(h->device));
+    unsigned long long* sink = nullptr;
+    ATB_CUDA(h, cudaMalloc(&sink, sizeof(unsigned long long)));
+    const int iters = 4096, grid = h->n_sm * 2;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    bench_smem_red_kernel<WIDE><<<grid, kBlock>>>(iters, pattern, sink);  // warm-up
+    cudaEventRecord(a);
+    for (int r = 0; r < 5; ++r) bench_smem_red_kernel<WIDE><<<grid, kBlock>>>(iters, pattern, sink);
+    cudaEventRecord(b);
+    cudaError_t e = cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(sink);
+    if (e != cudaSuccess) return fail(h, ATB_ECUDA, "bench: %s", cudaGetErrorString(e));
+    *reductions_per_s = 5.0 * grid * kBlock * (double)iters / (ms * 1e-3);
     return ATB_OK;
 }
 
@@ -2548,28 +2584,13 @@ int atb_plan_profile(atb_plan* p, void* stream, float* ms_stage, float* ms_searc
     return rc;
 }
 
+
 int atb_bench_smem_red_u64(atb_handle* h, int pattern, double* reductions_per_s) {
-    if (!h || !reductions_per_s) return ATB_EINVAL;
-    ATB_CUDA(h, cudaSetDevice(h->device));
-    unsigned long long* sink = nullptr;
-    ATB_CUDA(h, cudaMalloc(&sink, sizeof(unsigned long long)));
-    const int iters = 4096, grid = h->n_sm * 2;
-    cudaEvent_t a, b;
-    cudaEventCreate(&a);
-    cudaEventCreate(&b);
-    bench_smem_red_kernel<<<grid, kBlock>>>(iters, pattern, sink);  // warm-up
-    cudaEventRecord(a);
-    for (int r = 0; r < 5; ++r) bench_smem_red_kernel<<<grid, kBlock>>>(iters, pattern, sink);
-    cudaEventRecord(b);
-    cudaError_t e = cudaEventSynchronize(b);
-    float ms = 0;
-    cudaEventElapsedTime(&ms, a, b);
-    cudaEventDestroy(a);
-    cudaEventDestroy(b);
-    cudaFree(sink);
-    if (e != cudaSuccess) return fail(h, ATB_ECUDA, "bench: %s", cudaGetErrorString(e));
-    *reductions_per_s = 5.0 * grid * kBlock * (double)iters / (ms * 1e-3);
-    return ATB_OK;
+    return bench_smem_red<true>(h, pattern, reductions_per_s);
+}
+
+int atb_bench_smem_red_u32(atb_handle* h, int pattern, double* reductions_per_s) {
+    return bench_smem_red<false>(h, pattern, reductions_per_s);
 }
 
 int atb_bench_dfma(atb_handle* h, double* fma_per_s) {
@@ -2641,9 +2662,6 @@ struct StaticMeta {
     CurveStat stats[1];
 };
 static_assert(sizeof(StaticMeta) <= kStaticMetaBytes, "static metadata fits its slot");
-
-constexpr int kMaxStaticDevices = 64;
-std::atomic<unsigned char*> g_static_ptr[kMaxStaticDevices];
 
 // one-curve index arrays and the counters that must start at zero
 __global__ void static_meta_init(StaticMeta* m, long long n, long long n_periods, int nd,
@@ -2721,38 +2739,40 @@ extern "C" int atb_search_curve_static(const atb_params* prm, const double* t, c
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess)
         return static_fail(err, err_len, ATB_ECUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
-    if (dev < 0 || dev >= kMaxStaticDevices)
-        return static_fail(err, err_len, ATB_EINVAL, "device %d beyond the supported %d", dev,
-                           kMaxStaticDevices);
     int n_sm = 0, smem_optin = 0, smem_per_sm = 0;
-    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-    cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    cudaDeviceGetAttribute(&smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    e = cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess)
+        e = cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e == cudaSuccess)
+        e = cudaDeviceGetAttribute(&smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    if (e != cudaSuccess)
+        return static_fail(err, err_len, ATB_ECUDA, "cudaDeviceGetAttribute: %s",
+                           cudaGetErrorString(e));
     const int static_smem = (int)sizeof(GroupSmem) + 64;
     int dyn = std::min(smem_optin, smem_per_sm / kMinBlocks - 1024) - static_smem;
     dyn = dyn / 16 * 16;
     const int cap = dyn / 16;
 
-    // set-up, once per device: the scratch array's device address and the
-    // search kernels' shared-memory limit
-    unsigned char* base = g_static_ptr[dev].load(std::memory_order_acquire);
-    if (!base) {
-        void* ptr = nullptr;
-        e = cudaGetSymbolAddress(&ptr, g_static_scratch);
-        if (e != cudaSuccess || !ptr)
-            return static_fail(err, err_len, ATB_ECUDA, "cudaGetSymbolAddress: %s",
-                               cudaGetErrorString(e));
-        e = cudaFuncSetAttribute(search_kernel<ATB_GEOM_BINNED>,
+    // Set-up, with the device current: the scratch array's device address and
+    // the search kernels' shared-memory limit.  Both are taken again on every
+    // call (neither allocates), so a cudaDeviceReset or a recreated primary
+    // context between calls cannot leave a stale address or a lost limit.  The
+    // first call on a device also makes the runtime load this library's
+    // kernels and its scratch array onto that device.
+    void* ptr = nullptr;
+    e = cudaGetSymbolAddress(&ptr, g_static_scratch);
+    if (e != cudaSuccess || !ptr)
+        return static_fail(err, err_len, ATB_ECUDA, "cudaGetSymbolAddress: %s",
+                           cudaGetErrorString(e));
+    e = cudaFuncSetAttribute(search_kernel<ATB_GEOM_BINNED>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(search_kernel<ATB_GEOM_FIXED>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(search_kernel<ATB_GEOM_FIXED>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
-        if (e != cudaSuccess)
-            return static_fail(err, err_len, ATB_ECUDA, "cudaFuncSetAttribute: %s",
-                               cudaGetErrorString(e));
-        base = static_cast<unsigned char*>(ptr);
-        g_static_ptr[dev].store(base, std::memory_order_release);
-    }
+    if (e != cudaSuccess)
+        return static_fail(err, err_len, ATB_ECUDA, "cudaFuncSetAttribute: %s",
+                           cudaGetErrorString(e));
+    unsigned char* base = static_cast<unsigned char*>(ptr);
     double* sdt = reinterpret_cast<double*>(base + kOffDt);
     int* sqw = reinterpret_cast<int*>(base + kOffQw);
     int* sqy = reinterpret_cast<int*>(base + kOffQy);

@@ -13,7 +13,7 @@
  *       -> atb_run_gpu_bls(), or the batched plan API with ATB_GEOM_FIXED
  *   - search/v42_parity.py:27-107 run_vbls_exact_parity  +
  *     search/kernels/vbls_v42_parity.cu:12-181
- *       (the CuPy RawModule launch at v42_parity.py:253-261)
+ *       (the CuPy RawModule launch at v42_parity.py:79-87)
  *       -> atb_run_vbls_exact_parity(), or the plan API with ATB_GEOM_BINNED
  *   - search/api.py:27-140 BoxLeastSquaresGPU.power dispatches to the two
  *     above; its Python counterpart is astro_transit_gpu_b200.api.
@@ -189,9 +189,12 @@ int atb_plan_profile(atb_plan* p, void* stream, float* ms_stage, float* ms_searc
  * on the handle's device (each synchronises; a few milliseconds):
  *   atb_bench_smem_red_u64  64-bit shared-memory reductions per second
  *                           (pattern 0: conflict-free, 1: pseudo-random bins)
+ *   atb_bench_smem_red_u32  the same for 32-bit reductions, the width the
+ *                           search kernel's histogram words use
  *   atb_bench_dfma          FP64 fused multiply-adds per second
  */
 int atb_bench_smem_red_u64(atb_handle* h, int pattern, double* reductions_per_s);
+int atb_bench_smem_red_u32(atb_handle* h, int pattern, double* reductions_per_s);
 int atb_bench_dfma(atb_handle* h, double* fma_per_s);
 
 /*
@@ -209,7 +212,7 @@ int atb_run_gpu_bls(atb_handle* h, const double* t, const float* y, const float*
 /*
  * Multi-target parity path, the counterpart of run_vbls_exact_parity
  * (v42_parity.py:27) and its vbls_v42_parity_kernel launch
- * (v42_parity.py:253-261): n_targets curves of n_data points on one shared
+ * (v42_parity.py:79-87): n_targets curves of n_data points on one shared
  * time axis; flux and weights are [n_targets, n_data] row-major (weights NULL
  * = unit).  Outputs are [n_targets, n_periods]; best_index is a DEVICE array
  * of n_targets (or NULL).  max_bins = 0 disables the reference's cap.
@@ -247,12 +250,17 @@ int atb_debug_fold(atb_handle* h, const atb_params* params, const double* t, con
  * until the process exits.  Limits: at most ATB_STATIC_MAX_POINTS points, at
  * most 32 durations, and every period's bin count must fit the search kernel's
  * shared-memory histograms (larger ones are rejected; use the plan API).
- * Errors are written to err (err_len bytes, may be NULL); no exception, no
- * allocation on host or device.
+ * Errors are written to err (err_len bytes, may be NULL); no exception.  The
+ * call itself allocates nothing on host or device: it calls no cudaMalloc,
+ * cudaFree or allocating library routine.
  *
- * The call is synchronous on `stream`.  The first call on a device looks up
- * the array's device address and sets the kernels' shared-memory limit; make
- * that first call before any stream capture.  Every call uses the same array
+ * The call is synchronous on `stream`.  Each call looks up the array's device
+ * address and sets the kernels' shared-memory limit (neither allocates).  With
+ * CUDA's lazy module loading, the first call on a device is the one that makes
+ * the runtime load this library's kernels and map the array on that device,
+ * which may allocate and synchronise inside the driver: make that first call
+ * at start-up (a call with n = 1 is enough) and before any stream capture;
+ * from the second call on nothing is loaded or mapped.  Every call uses the same array
  * (the previous call's contents remain; the call resets what must start at
  * zero), so calls on the same device must not overlap on the GPU: concurrent
  * calls from several streams or threads race and corrupt each other's results.

@@ -72,10 +72,11 @@ def expected_bits(t, periods, durs, cfg):
         return 64
     if cfg.method == "fast":
         width = periods.max() / cfg.n_bins
-    elif cfg.max_bins:
-        return 64
     else:
         width = durs.min() / cfg.oversample
+        # a bin cap that the largest period reaches piles points into its last bin
+        if cfg.max_bins and np.ceil(periods.max() * (1 / width)) + cfg.oversample >= cfg.max_bins:
+            return 64
     width = width * (1 + 1e-6) + 1e-12
     k = int((np.searchsorted(t, t + width, side="right") - np.arange(t.size)).max())
     m = (np.floor((t[-1] - t[0]) * (1 / periods).max() * (1 + 1e-9)) + 3) * k
@@ -103,13 +104,18 @@ CASES = {
                           np.array([0.04, 0.1]), "binned", None, TIGHT),
     "clustered_fixed": lambda: (*clustered(seed=5), None, np.geomspace(0.5, 13.7, 500),
                                 np.array([0.04, 0.1]), "fixed", 2000, TIGHT),
+    # the reference's default cap (max_bins=2000) where no period reaches it:
+    # 0.004 d bins up to 7.9 d need at most 1985 bins
+    "c0_uniform_cap_not_reached": lambda: (*R.c0_curve(n=15000, seed=2)[:2], None,
+                                           R.c0_periods(600, pmax=7.9), R.C0_DURATIONS,
+                                           "binned", 2000, TIGHT),
 }
 
 
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_tight_layout_bound_holds_and_results_bit_exact(engine, name):
     t, y, w, periods, durs, kind, n_bins, expect = CASES[name]()
-    cfg = _cfg(kind, n_bins=n_bins)
+    cfg = _cfg(kind, n_bins=n_bins, max_bins=n_bins if kind == "binned" else None)
     g, lay, bits = run_with_layout(engine, t, y, w, periods, durs, cfg)
     assert lay == expect, (lay, bits)
     assert bits == expected_bits(t, periods, durs, cfg) <= 12
@@ -130,8 +136,8 @@ def test_layout_falls_back_when_no_bound(engine):
         # unsorted times: no bound is computed
         (rng.permutation(R.c0_curve(n=4000, seed=4)[0]), rng.normal(1, 1e-3, 4000), None,
          "binned", None, COUNT),
-        # the reference's bin cap folds many points into the last bin
-        (*R.c0_curve(n=4000, seed=4)[:2], None, "binned", 2000, COUNT),
+        # a bin cap that the grid reaches folds many points into the last bin
+        (*R.c0_curve(n=4000, seed=4)[:2], None, "binned", 500, COUNT),
         # non-uniform weights
         (*R.c0_curve(n=4000, seed=4)[:2], rng.uniform(1e5, 2e5, 4000).astype(np.float32),
          "binned", None, SPLIT),

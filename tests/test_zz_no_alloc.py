@@ -31,8 +31,9 @@ def _ptr(x):
     return None if x is None else ctypes.c_void_p(x.data_ptr())
 
 
-def call_static(t, y, w, periods, durations, cfg):
-    """One call of atb_search_curve_static on cuda:0; returns host outputs."""
+def call_static(t, y, w, periods, durations, cfg, with_best=True):
+    """One call of atb_search_curve_static on cuda:0; returns host outputs
+    (best_index is -7 when the call is made without a best-index output)."""
     dev = torch.device("cuda", 0)
     tt = torch.tensor(np.asarray(t, np.float64), device=dev)
     yy = torch.tensor(np.asarray(y), device=dev)
@@ -46,7 +47,7 @@ def call_static(t, y, w, periods, durations, cfg):
     rc = N.load().atb_search_curve_static(
         ctypes.byref(prm), _ptr(tt), _ptr(yy), 1 if yy.dtype == torch.float64 else 0, _ptr(ww),
         tt.numel(), _ptr(pp), pp.numel(), _ptr(dd), dd.numel(),
-        *(_ptr(out[k]) for k in FIELDS), _ptr(best),
+        *(_ptr(out[k]) for k in FIELDS), _ptr(best) if with_best else None,
         ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream), err, len(err))
     host = {k: v.cpu().numpy() for k, v in out.items()}
     host["best_index"] = int(best.item())
@@ -102,3 +103,31 @@ def test_static_entry_rejects_what_exceeds_its_scratch():
     t = np.linspace(0.0, 30.0, 1000)
     rc, msg, _ = call_static(t, np.ones(1000, np.float32), None, [25.0], [0.001], cfg)
     assert rc == N.ATB_EINVAL and "bins" in msg
+
+
+def test_static_entry_recovers_from_invalid_data_and_runs_without_best_index():
+    """A call that meets a NaN flux reports ATB_EDATA; the shared array still
+    serves the next call, which matches the plan API bit for bit.  That call
+    passes no best-index output, and its grid has more work-queue tiles than
+    the launch has CTAs (every CTA takes several tiles)."""
+    cfg = SearchConfig("parity", objective="snr")
+    t, y, dy = R.c0_curve(n=4000, seed=12)
+    y32 = y.astype(np.float32)
+    w = (1.0 / dy ** 2).astype(np.float32)
+    bad = y32.copy()
+    bad[1234] = np.nan
+    rc, msg, _ = call_static(t, bad, w, R.c0_periods(300), R.C0_DURATIONS, cfg)
+    assert rc == N.ATB_EDATA and "non-finite" in msg
+    # 40 000 periods: 625 tiles of 64 against at most 2 CTAs per SM
+    periods = np.geomspace(0.5, 13.7, 40000)
+    rc, msg, got = call_static(t, y32, w, periods, R.C0_DURATIONS, cfg, with_best=False)
+    assert rc == N.ATB_OK, msg
+    assert got["best_index"] == -7  # nothing was written there
+    ref = call_plan(t, y32, w, periods, R.C0_DURATIONS, cfg)
+    got["best_index"] = ref["best_index"]
+    assert_same(got, ref, "after invalid data")
+    # and a fixed-bin call after it, with the best index, still agrees
+    cfg2 = SearchConfig("fast", n_bins=200)
+    rc, msg, got2 = call_static(t, y32, w, R.c0_periods(500), R.C0_DURATIONS, cfg2)
+    assert rc == N.ATB_OK, msg
+    assert_same(got2, call_plan(t, y32, w, R.c0_periods(500), R.C0_DURATIONS, cfg2), "fixed")
