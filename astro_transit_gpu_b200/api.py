@@ -10,9 +10,11 @@ Behavioural differences from the reference, all deliberate:
 
 * the fold runs in FP64 and bin sums in exact 64-bit fixed point whatever
   ``dtype`` says (``dtype`` only sets the dtype of the returned arrays);
-* ``method="parity"`` does not cap the bin count unless ``max_bins`` is passed
-  explicitly (the reference silently caps at ``max_bins-1 = 1999`` bins,
-  vbls_v42_parity.cu:46-47); pass ``max_bins=2000`` to reproduce that;
+* ``method="parity"`` caps the bin count at ``max_bins - 1`` with the
+  reference's default ``max_bins=2000`` (vbls_v42_parity.cu:46-47), so a
+  reference caller gets the reference's results; above 7.96 d with 0.004 d
+  bins that cap distorts the spectrum, and ``max_bins=None`` (or 0) searches
+  every period with its full bin count instead;
 * exact ties between windows go to the lowest start bin, then the lowest
   duration index.
 """
@@ -88,9 +90,10 @@ def _validate(t, y, dy, periods, durations):
 
 def _config(method: str, n_bins: int, kwargs: Dict[str, Any]) -> SearchConfig:
     if method == "parity":
+        max_bins = kwargs.get("max_bins", 2000)  # the reference's default, api.py:75
         return SearchConfig(method="parity", objective=kwargs.get("objective", "snr"),
                             oversample=int(kwargs.get("oversample", 10)),
-                            max_bins=kwargs.get("max_bins", None))
+                            max_bins=int(max_bins) if max_bins else None)
     if method == "fast":
         if kwargs.get("objective", "fast") != "fast":
             raise ValueError("method='fast' has a single objective; use method='parity'")
@@ -115,7 +118,9 @@ def _result(periods, out, cfg: SearchConfig, dtype, n_data: int, orig_periods,
         top = [Candidate(float(c["period"]), float(c["t0"]), float(c["duration"]),
                          float(c["depth"]), float(c["power"]))
                for c in get_top_k_candidates(raw, k=5)]
+    # the reference reports max_bins as n_bins for the parity method (api.py:103)
     meta = {"n_bins": cfg.n_bins if cfg.method == "fast" else cfg.max_bins,
+            "max_bins": cfg.max_bins if cfg.method == "parity" else None,
             "dtype": str(dtype), "n_data": n_data, "method": cfg.method,
             "objective": cfg.objective or ("fast" if cfg.method == "fast" else "snr"),
             "oversample": cfg.oversample if cfg.method == "parity" else None,
@@ -144,7 +149,8 @@ class BoxLeastSquaresGPU:
 
         method="fast"   fixed ``n_bins`` phase bins, two-sided score (bls.cu)
         method="parity" Astropy-style bins of min(durations)/oversample; kwargs
-                        ``oversample`` (10), ``max_bins`` (None = no cap),
+                        ``oversample`` (10), ``max_bins`` (2000 as the
+                        reference: at most 1999 bins; None or 0 = no cap),
                         ``objective`` ("snr" as the reference, or "likelihood")
         """
         orig = periods

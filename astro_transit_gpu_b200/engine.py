@@ -313,7 +313,12 @@ class BLSEngine:
                            torch.device(device).index or 0)
         self.device = dev
         self.handle = N.Handle(dev.index)
-        self._tuned: Dict[tuple, int] = {}  # tune_key -> tile periods (autotune)
+        from .tuning import TuningTable, table_path
+        name = torch.cuda.get_device_name(dev)
+        # settings BLSEngine.autotune found for kinds of batch on this kind of
+        # device, persisted across processes
+        self.tuning = TuningTable(table_path(name, torch.cuda.get_device_capability(dev)), name,
+                                  self.handle.lib.atb_version().decode()).load()
         self.last_tune: Dict[int, float] = {}
 
     @classmethod
@@ -327,12 +332,16 @@ class BLSEngine:
 
     def bench_peaks(self) -> Dict[str, float]:
         """Measured denominators of the search kernel's roofline on this device:
-        64-bit shared-memory reductions/s (conflict-free and random bins) and
-        FP64 fused multiply-adds/s."""
+        32- and 64-bit shared-memory reductions/s (conflict-free and random
+        bins) and FP64 fused multiply-adds/s."""
         out = {}
         v = ctypes.c_double(0.0)
-        for name, pat in (("smem_red_u64_per_s", 0), ("smem_red_u64_random_per_s", 1)):
-            rc = self.handle.lib.atb_bench_smem_red_u64(self.handle.ptr, pat, ctypes.byref(v))
+        lib = self.handle.lib
+        for name, fn, pat in (("smem_red_u32_per_s", lib.atb_bench_smem_red_u32, 0),
+                              ("smem_red_u32_random_per_s", lib.atb_bench_smem_red_u32, 1),
+                              ("smem_red_u64_per_s", lib.atb_bench_smem_red_u64, 0),
+                              ("smem_red_u64_random_per_s", lib.atb_bench_smem_red_u64, 1)):
+            rc = fn(self.handle.ptr, pat, ctypes.byref(v))
             N.raise_for(rc, self.handle.ptr, "smem benchmark")
             out[name] = v.value
         rc = self.handle.lib.atb_bench_dfma(self.handle.ptr, ctypes.byref(v))
@@ -361,11 +370,13 @@ class BLSEngine:
         return (config.method, b(nc), b(pts), b(per))
 
     def autotune(self, batch: CurveBatch, config: SearchConfig,
-                 candidates: Sequence[int] = (8, 16, 32, 64), repeats: int = 2) -> int:
+                 candidates: Sequence[int] = (8, 16, 32, 64), repeats: int = 2,
+                 persist: bool = True) -> int:
         """Time the search kernel on `batch` for each tile size in `candidates`
         (results are identical for all), keep the fastest for this kind of
-        batch (``tune_key``) and return it; later plans with
-        ``tile_periods == 0`` use it."""
+        batch (``tune_key``) in the engine's tuning table -- written to its
+        file unless `persist` is false -- and return it; later plans with
+        ``tile_periods == 0`` use it, in this process and in later ones."""
         times = {}
         for tp in candidates:
             cfg = SearchConfig(config.method, config.objective, config.n_bins, config.oversample,
@@ -378,7 +389,11 @@ class BLSEngine:
             finally:
                 plan.close()
         best = min(times, key=times.get)
-        self._tuned[self.tune_key(batch, config)] = best
+        self.tuning.put(self.tune_key(batch, config),
+                        {"tile_periods": int(best),
+                         "search_ms": {str(k): float(v) for k, v in times.items()}})
+        if persist:
+            self.tuning.save()
         self.last_tune = times
         return best
 
@@ -388,10 +403,11 @@ class BLSEngine:
         if outputs is None:
             outputs = self.allocate_outputs(batch)
         if config.tile_periods == 0:
-            tp = self._tuned.get(self.tune_key(batch, config))
-            if tp is not None:
+            tuned = self.tuning.get(self.tune_key(batch, config))
+            if tuned is not None and "tile_periods" in tuned:
                 config = SearchConfig(config.method, config.objective, config.n_bins,
-                                      config.oversample, config.max_bins, tp)
+                                      config.oversample, config.max_bins,
+                                      int(tuned["tile_periods"]))
         return SearchPlan(self, batch, config, outputs, stream)
 
     def screen(self, batch: CurveBatch, config: SearchConfig,

@@ -18,13 +18,18 @@ formulas), so a request gets the same result alone and in any mix.
 
 Latency is measured per request from ``submit`` to the moment its result is
 ready; :meth:`BLSServer.stats` reports p50/p99 and the completed rate.
+
+A request can carry a timeout: if it is still waiting for admission when the
+timeout has passed, it is dropped and its future raises ``TimeoutError``.  A
+client can also ``cancel()`` its future while the request waits; an admitted
+request runs to completion (its batch is already on the GPU).
 """
 from __future__ import annotations
 
 import threading
 import time
 from collections import deque
-from concurrent.futures import Future
+from concurrent.futures import Future, InvalidStateError
 from dataclasses import dataclass, field
 from typing import Dict, List, Optional
 
@@ -47,6 +52,7 @@ class _Request:
     arrival: float
     future: Future = field(default_factory=Future)
     done: float = 0.0
+    deadline: Optional[float] = None  # admission deadline (perf_counter seconds)
 
 
 @dataclass(eq=False)
@@ -82,6 +88,21 @@ def admit(pending, key, held: int, budget: int, max_batch: int):
     return take, rest, used
 
 
+def prune(pending, now: float):
+    """Split the waiting requests into those that keep waiting (in arrival
+    order), those whose admission deadline has passed, and those whose client
+    cancelled them."""
+    keep, expired, cancelled = deque(), [], []
+    for r in pending:
+        if r.future.cancelled():
+            cancelled.append(r)
+        elif r.deadline is not None and now > r.deadline:
+            expired.append(r)
+        else:
+            keep.append(r)
+    return keep, expired, cancelled
+
+
 def request_bytes(n_points: int, n_periods: int, n_durations: int) -> int:
     """Device bytes a request holds while its batch runs: inputs (t f64, y, w
     f32), staged points (16 B), the grids and the per-period outputs (28 B),
@@ -114,15 +135,21 @@ class BLSServer:
         self._t_last: Optional[float] = None
         self._batches = 0
         self._max_held = 0
+        self._expired = 0
+        self._cancelled = 0
         self._worker = threading.Thread(target=self._run, name="bls-server", daemon=True)
         self._worker.start()
 
     # ---------------------------------------------------------------- client
     def submit(self, t, y, dy=None, periods=None, durations=None, method: str = "fast",
                n_bins: int = 200, objective: Optional[str] = None, oversample: int = 10,
-               max_bins: Optional[int] = None) -> Future:
+               max_bins: Optional[int] = None, timeout: Optional[float] = None) -> Future:
         """Queue one search; the future resolves to the curve's per-period
-        outputs (power, depth, depth_err, t0, duration, window) and best_index."""
+        outputs (power, depth, depth_err, t0, duration, window) and best_index.
+        `timeout` (seconds): if the request is still waiting for admission
+        that long after submission, it is dropped and the future raises
+        TimeoutError.  Cancelling the future while the request waits drops it
+        too."""
         if periods is None or durations is None:
             raise ValueError("periods and durations must be given")
         t = np.ascontiguousarray(t, np.float64)
@@ -143,8 +170,10 @@ class BLSServer:
         cfg.params()  # validates the combination
         per = np.atleast_1d(np.asarray(periods, np.float64))
         dur = np.atleast_1d(np.asarray(durations, np.float64))
+        now = time.perf_counter()
         req = _Request(t, y, w, per, dur, cfg, fdt,
-                       request_bytes(len(t), len(per), len(dur)), time.perf_counter())
+                       request_bytes(len(t), len(per), len(dur)), now,
+                       deadline=None if timeout is None else now + float(timeout))
         if req.nbytes > self.memory_budget:
             raise MemoryError(f"request needs {req.nbytes} bytes, budget {self.memory_budget}")
         with self._cv:
@@ -165,6 +194,7 @@ class BLSServer:
                 "mean_ms": float(lat.mean() * 1e3) if lat.size else float("nan"),
                 "curves_per_s": float(lat.size / span) if span > 0 else float("nan"),
                 "max_held_bytes": self._max_held,
+                "expired": self._expired, "cancelled": self._cancelled,
             }
 
     def reset_stats(self) -> None:
@@ -174,6 +204,7 @@ class BLSServer:
             self._latencies.clear()
             self._t_first = self._t_last = None
             self._batches = 0
+            self._expired = self._cancelled = 0
 
     def close(self) -> None:
         """Finish every submitted request, then stop the worker."""
@@ -198,8 +229,16 @@ class BLSServer:
     def _admit(self) -> List[_Request]:
         take, self._pending, self._held = admit(self._pending, self._key, self._held,
                                                 self.memory_budget, self.max_batch)
+        # from here on a request runs; one cancelled a moment ago is dropped
+        run = []
+        for r in take:
+            if r.future.set_running_or_notify_cancel():
+                run.append(r)
+            else:
+                self._held -= r.nbytes
+                self._cancelled += 1
         self._max_held = max(self._max_held, self._held)
-        return take
+        return run
 
     def _launch(self, reqs: List[_Request], stream: torch.cuda.Stream) -> _Batch:
         with torch.cuda.stream(stream):
@@ -259,6 +298,16 @@ class BLSServer:
             for b in [b for b in self._inflight if b.event.query()]:
                 self._inflight.remove(b)
                 self._finish(b)
+            with self._cv:
+                self._pending, expired, cancelled = prune(self._pending, time.perf_counter())
+                self._expired += len(expired)
+                self._cancelled += len(cancelled)
+            for r in expired:
+                try:
+                    r.future.set_exception(TimeoutError(
+                        "request not admitted within its timeout"))
+                except InvalidStateError:  # cancelled by its client meanwhile
+                    pass
             with self._cv:
                 busy = {id(b.stream) for b in self._inflight}
                 free = [s for s in self.streams if id(s) not in busy]

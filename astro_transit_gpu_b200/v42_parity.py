@@ -1,9 +1,10 @@
 """``run_vbls_exact_parity``: the reference's multi-target parity-path host
 function (search/v42_parity.py:27-107), backed by the B200 engine.
 
-``flux_matrix`` is [n_targets, n_data] on the shared ``time_array``.  Unlike
-the reference, ``max_bins`` defaults to None (no cap); pass the reference's
-2000 to reproduce its capped bin count.
+``flux_matrix`` is [n_targets, n_data] on the shared ``time_array``.
+``max_bins`` defaults to the reference's 2000 (at most 1999 bins per period,
+vbls_v42_parity.cu:46-47); None or 0 searches every period with its full bin
+count.
 """
 from __future__ import annotations
 
@@ -11,7 +12,7 @@ import numpy as np
 
 
 def run_vbls_exact_parity(time_array, flux_matrix, periods, durations, weights_matrix=None,
-                          oversample=10, max_bins=None, dtype=None, objective="snr"):
+                          oversample=10, max_bins=2000, dtype=None, objective="snr"):
     from .engine import BLSEngine, CurveBatch, SearchConfig
 
     flux = np.asarray(flux_matrix)
@@ -36,7 +37,7 @@ def run_vbls_exact_parity(time_array, flux_matrix, periods, durations, weights_m
                                    periods=periods, durations=durations, flux_dtype=fdt,
                                    weights=weights)
     cfg = SearchConfig("parity", objective=objective, oversample=int(oversample),
-                       max_bins=max_bins)
+                       max_bins=int(max_bins) if max_bins else None)
     out = BLSEngine.get().search(batch, cfg)
     host = {k: v.cpu().numpy() for k, v in out.items()}
     odt = np.float64 if dtype is not None and np.dtype(dtype) == np.float64 else np.float32

@@ -511,7 +511,7 @@ def test_screen_equals_full_search_at_its_best_period(engine, method):
 
 # ------------------------------------------------------------ autotuning ---
 
-def test_tile_size_never_changes_results_and_autotune_picks_one(engine):
+def test_tile_size_never_changes_results_and_autotune_picks_one(engine, tmp_path):
     """Every tile size (periods per work-queue tile) gives bit-identical
     outputs; the autotuner times the candidates and later plans of the same
     kind of batch use the winner."""
@@ -529,6 +529,21 @@ def test_tile_size_never_changes_results_and_autotune_picks_one(engine):
         for k in ref:
             assert np.array_equal(out[k], ref[k]), (tp, k)
     cfg = SearchConfig("parity", objective="likelihood")
-    best = engine.autotune(b, cfg, candidates=(8, 64))
-    assert best in (8, 64) and set(engine.last_tune) == {8, 64}
-    assert engine._tuned[engine.tune_key(b, cfg)] == best
+    from astro_transit_gpu_b200.tuning import TuningTable
+    saved = engine.tuning
+    engine.tuning = TuningTable(str(tmp_path / "tuning.json"), saved.device_name,
+                                saved.library)
+    try:
+        best = engine.autotune(b, cfg, candidates=(8, 64))
+        assert best in (8, 64) and set(engine.last_tune) == {8, 64}
+        key = engine.tune_key(b, cfg)
+        assert engine.tuning.get(key)["tile_periods"] == best
+        # persisted: a table read back from the file holds the same setting
+        again = TuningTable(engine.tuning.path, saved.device_name, saved.library).load()
+        assert again.get(key)["tile_periods"] == best
+        # the tuned plan gives what the default plan gave
+        out = {k: v.cpu().numpy() for k, v in engine.search(b, cfg).items()}
+        for k in ref:
+            assert np.array_equal(out[k], ref[k]), k
+    finally:
+        engine.tuning = saved

@@ -64,3 +64,31 @@ def test_budget_forces_small_batches_and_results_still_match(engine):
         ref = _alone(engine, r)
         for k in FIELDS:
             assert np.array_equal(g[k], ref[k]), k
+
+
+def test_timeout_and_cancellation_before_admission(engine):
+    """One stream and one request per batch: while a large request runs, a
+    request with a tiny timeout expires in the queue (TimeoutError) and a
+    cancelled one never runs; a later request without a timeout completes
+    with the same result as alone."""
+    import concurrent.futures as cf
+    from astro_transit_gpu_b200.serving import BLSServer
+    rng = np.random.default_rng(17)
+    big_t, big_y, big_dy, big_p = R.mixed_curve(rng, 13, R.CADENCE_2MIN, 150000, 40000)
+    small = _requests(n=2, seed=23)
+    with BLSServer(max_batch=1, n_streams=1) as srv:
+        f_big = srv.submit(big_t, big_y, big_dy, periods=big_p, durations=R.C2_DURATIONS)
+        f_exp = srv.submit(**small[0], timeout=1e-6)
+        f_can = srv.submit(**small[0])
+        cancelled = f_can.cancel()
+        f_ok = srv.submit(**small[1])
+        f_big.result(timeout=300)
+        with pytest.raises(cf.TimeoutError):
+            f_exp.result(timeout=300)
+        got = f_ok.result(timeout=300)
+        st = srv.stats()
+    assert cancelled and f_can.cancelled()
+    assert st["expired"] == 1 and st["cancelled"] == 1 and st["completed"] == 2
+    ref = _alone(engine, small[1])
+    for k in FIELDS:
+        assert np.array_equal(got[k], ref[k]), k

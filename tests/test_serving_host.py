@@ -43,3 +43,16 @@ def test_admit_waits_when_the_head_does_not_fit():
 
 def test_request_bytes_grows_with_the_request():
     assert request_bytes(1000, 100, 4) < request_bytes(2000, 100, 4) < request_bytes(2000, 200, 4)
+
+
+def test_prune_drops_expired_and_cancelled_requests_in_order():
+    from concurrent.futures import Future
+    from astro_transit_gpu_b200.serving import prune
+    P = namedtuple("P", "name future deadline")
+    a, b, c, d = (P("a", Future(), None), P("b", Future(), 5.0), P("c", Future(), 20.0),
+                  P("d", Future(), None))
+    assert c.future.cancel()
+    keep, expired, cancelled = prune([a, b, c, d], now=10.0)
+    assert names(keep) == ["a", "d"] and names(expired) == ["b"] and names(cancelled) == ["c"]
+    keep, expired, cancelled = prune([a, b, d], now=1.0)
+    assert names(keep) == ["a", "b", "d"] and not expired and not cancelled

@@ -1,0 +1,32 @@
+"""The persisted autotuning table: round trip through its JSON file, and files
+written for another device or library version are ignored (no GPU needed)."""
+import json
+
+from astro_transit_gpu_b200.tuning import TuningTable, key_str, table_path
+
+
+def test_table_round_trip(tmp_path):
+    path = table_path("NVIDIA B200", (10, 0), str(tmp_path))
+    assert path.endswith("tuning-NVIDIA_B200-sm100.json")
+    t = TuningTable(path, "NVIDIA B200", "lib 1").load()
+    assert t.get(("fast", 13, 14, 15)) is None
+    t.put(("fast", 13, 14, 15), {"tile_periods": 32, "search_ms": {"8": 2.0, "32": 1.5}})
+    t.put(("parity", 12, 13, 12), {"tile_periods": 64})
+    t.save()
+    u = TuningTable(path, "NVIDIA B200", "lib 1").load()
+    assert u.get(("fast", 13, 14, 15)) == {"tile_periods": 32, "search_ms": {"8": 2.0, "32": 1.5}}
+    assert u.get(("parity", 12, 13, 12))["tile_periods"] == 64
+    assert json.load(open(path))["entries"][key_str(("parity", 12, 13, 12))]["tile_periods"] == 64
+
+
+def test_table_ignores_other_devices_versions_and_bad_files(tmp_path):
+    path = str(tmp_path / "t.json")
+    t = TuningTable(path, "NVIDIA B200", "lib 1")
+    t.put(("fast", 1, 2, 3), {"tile_periods": 8})
+    t.save()
+    assert TuningTable(path, "NVIDIA B200", "lib 2").load().get(("fast", 1, 2, 3)) is None
+    assert TuningTable(path, "Other GPU", "lib 1").load().get(("fast", 1, 2, 3)) is None
+    with open(path, "w") as f:
+        f.write("{not json")
+    assert TuningTable(path, "NVIDIA B200", "lib 1").load().entries == {}
+    assert TuningTable(str(tmp_path / "missing.json"), "x", "y").load().entries == {}
