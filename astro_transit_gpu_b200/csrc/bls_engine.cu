@@ -64,6 +64,7 @@ constexpr int kMaxG = 64;              // periods per shared-memory group
 constexpr int kMaxDur = 32;            // durations per curve
 constexpr int kStageAlign = 32;        // staged curves start at multiples of 32 points
 constexpr int kStageBlock = 256;
+constexpr double kDefaultMergeRun = 8.0;   // atb_params.merge_run = 0
 constexpr int kChunk = 32 * kR;        // staged points of one warp's fold step
 constexpr double kMagicSlot = 4503599627370497.0;   // 2^52 + 1: x + C (rz) = 2^52 + int(x) + 1, x in (-1, 2^31 - 1)
 constexpr double kMagicFloor = 6755399441055744.0;  // 1.5*2^52: (m + C)(rd) - C = floor(m), |m| < 2^50
@@ -81,10 +82,21 @@ constexpr double kMagicFloor = 6755399441055744.0;  // 1.5*2^52: (m + C)(rd) - C
 //               of one bin in one cycle lie in such a window, and the rounded
 //               cycle index takes at most floor(T / P) + 2 values.  High words
 //               sum to < M * 2^(26 - lobits) <= 2^(3b - 6) <= 2^30.
+//   Checked tight: uniform weights with no proven bound, but few points per bin
+//               on average (below kCheckedTightAvg per real bin at the grid's
+//               coarsest binning): the tight words with b = 12, and every
+//               period's histogram checked before use -- a count field that
+//               overflowed (a bin holding 2^12 points or more) makes the decoded
+//               counts sum to less than n (each such bin loses at least
+//               2^12 - 1 points while carries add at most 1), and that period
+//               is folded again in the count layout (kPackCountT), whose words
+//               are derived from the same staged tight words.
 constexpr int kPackSplit = 0;
 constexpr int kPackCount = 1;
 constexpr int kPackTight = 2;
+constexpr int kPackCountT = 3;  // count-layout words computed from staged tight words
 constexpr int kTightMaxBits = 12;
+constexpr double kCheckedTightAvg = 1024.0;
 
 // Per-curve fixed-point layout.  Point values are quantised to |q| <= 2^qbits;
 // histogram words hold the low `lobits` bits and the arithmetic-shifted high
@@ -120,6 +132,10 @@ struct CurveStat {
                     // works on exact FP32 point counts instead of FP64 weight sums
     int n_cnt;      // number of points (cnt_win)
     int ilv;        // staged order interleaved within whole chunks (staged_pos)
+    double density; // points per unit time, (n - 1) / (time span); 0 for n < 2
+    int tcheck;     // kPackTight without a proven bound: each period's counts are checked
+    int stage_lob;  // kPackTight: low flux bits of the staged word x (32 - 2b)
+    int stage_csh;  // kPackTight: bit position of the count in the staged word x (32 - b)
 };
 
 struct StageArgs {
@@ -184,6 +200,7 @@ struct SearchArgs {
     int* status;
     unsigned long long* best_key;  // winner-take-all per-curve records (or NULL)
     int tile_p;                    // periods per work-queue tile (1..kTileP)
+    double merge_run;              // expected points per bin from which kFoldChunk is used
 };
 
 // ----------------------------------------------------------------------------
@@ -388,6 +405,40 @@ __device__ int occupancy_bits(const StageArgs& a, int c, const double* t, long l
     return bitlen64((long long)m);
 }
 
+// Whether curve c may use the checked tight layout: fewer than
+// kCheckedTightAvg points per real bin on average at the grid's coarsest
+// binning (fixed: n_bins; astropy-binned: the bins of the smallest period),
+// and, for astropy bins, a bin cap (max_bins) that no period reaches (the cap
+// piles points into the last bin).  Bins far fuller than the average only cost
+// a second fold of their period.
+__device__ bool checked_tight_ok(const StageArgs& a, int c, long long n, double* shd) {
+    const double* per = a.periods + a.per_beg[c];
+    const long long np = a.per_cnt[c];
+    double pmax = 0.0, pinv = 0.0;
+    for (long long i = threadIdx.x; i < np; i += kStageBlock) {
+        const double P = per[i];
+        if (P > 0.0 && P < 1.0e300) {
+            pmax = max(pmax, P);
+            pinv = max(pinv, 1.0 / P);
+        }
+    }
+    pmax = block_max_d(pmax, shd);
+    pinv = block_max_d(pinv, shd);
+    if (!(pinv > 0.0)) return false;
+    double real_bins = (double)a.n_bins_fixed;
+    if (a.geometry == ATB_GEOM_BINNED) {
+        const double* dur = a.durations + a.dur_beg[c];
+        double min_dur = dur[0];
+        for (int k = 1; k < a.dur_cnt[c]; ++k) min_dur = min(min_dur, dur[k]);
+        const double ibd = 1.0 / (min_dur / (double)a.oversample);
+        if (!(ibd > 0.0) || !isfinite(ibd)) return false;
+        if (a.max_bins > 0 && binned_nbins(pmax, ibd, a.oversample, 0) >= a.max_bins)
+            return false;
+        real_bins = (double)(binned_nbins(1.0 / pinv, ibd, a.oversample, 0) - a.oversample);
+    }
+    return real_bins >= 1.0 && (double)n < kCheckedTightAvg * real_bins;
+}
+
 template <typename YT>
 __global__ void __launch_bounds__(kStageBlock) stage_kernel(const StageArgs a) {
     __shared__ double shd[kStageBlock / 32];
@@ -444,6 +495,14 @@ __global__ void __launch_bounds__(kStageBlock) stage_kernel(const StageArgs a) {
     int tight_bits = 64;
     if (uniform && a.periods) tight_bits = occupancy_bits(a, c, t, n, shd, shl);
     if (uniform && tight_bits <= kTightMaxBits && qbits <= 26) packmode = kPackTight;
+    // no proven bound: the checked tight layout where bins are sparse on average
+    bool tcheck = false;
+    if (uniform && packmode != kPackTight && a.periods && qbits <= 26 && n < (1LL << 24) &&
+        checked_tight_ok(a, c, n, shd)) {
+        packmode = kPackTight;
+        tight_bits = kTightMaxBits;
+        tcheck = true;
+    }
     const int qbits_y = qbits;
     const double shift = sqw != 0 ? ldexp((double)sqa / (double)sqw, s_w - s_a) : 0.0;
 
@@ -547,10 +606,14 @@ __global__ void __launch_bounds__(kStageBlock) stage_kernel(const StageArgs a) {
         } else {
             st.cshift = 0;
         }
-        st.occ_bits = tight_bits;
+        st.occ_bits = tcheck ? 64 : tight_bits;
+        st.tcheck = tcheck ? 1 : 0;
+        st.stage_lob = packmode == kPackTight ? 32 - 2 * tight_bits : 0;
+        st.stage_csh = packmode == kPackTight ? 32 - tight_bits : 0;
         st.cnt_win = (uniform && n < (1LL << 24)) ? 1 : 0;
         st.n_cnt = st.cnt_win ? (int)n : 0;
         st.ilv = ilv ? 1 : 0;
+        st.density = (n > 1 && tmax > 0.0) ? (double)(n - 1) / tmax : 0.0;
         a.stats[c] = st;
     }
 }
@@ -622,6 +685,9 @@ struct GroupSmem {
     int tNB[kTileP];     // and their bin counts
     double2 PIP[kMaxG];  // (P, 1/P) of each period of the group
     int2 NBB[kMaxG];     // (bin count, histogram offset) of each period
+    int fmode[kMaxG];    // fold mode of each period (kFold*)
+    int redo[kMaxG];     // checked tight layout: the period's counts overflowed
+    int n_redo;          // how many periods of the group are folded again
     long long slot[kMaxG];
     int dbins[kMaxDur];
     double dur[kMaxDur];
@@ -747,17 +813,61 @@ __device__ __forceinline__ void hist_add_point(unsigned base0, uint4* H0, unsign
     }
 }
 
-// Fold every staged point of the curve into the group's histograms: one
-// reduction per histogram word and point (merging runs of equal bins costs
-// more issue slots than the reductions it saves).
+// Fold modes, chosen per period from the expected number of time-ordered
+// points that share a bin (bin width x the curve's mean point density):
+//   kFoldPoint  one reduction per histogram word and point
+//   kFoldChunk  a lane whose kR points provably share one slot (fold_ends)
+//               adds their summed words once; other lanes as kFoldPoint
+// The histogram words are integers added modulo 2^32, so both modes give the
+// same sums, bit for bit; they differ only in how many reductions reach shared
+// memory.  With few points per bin the per-point form is cheapest (the check
+// costs issue slots and rarely saves a reduction); with several, neighbouring
+// lanes add to the same address, and same-address reductions serialise.
+// (Merging equal slots across the lanes of a warp as well, with a segmented
+// shuffle scan, measured slower on every workload: the shuffles cost more of
+// the shared-memory pipe than the reductions they save.)
+constexpr int kFoldPoint = 0;
+constexpr int kFoldChunk = 1;
+
+// Slot of a lane's first point and whether all kR points share it, in the fast
+// fold form of fold_slots (the caller checked `safe`): the points are
+// time-ordered and lie in one cycle (the same k = floor(d*IP)), where the
+// slot is a non-decreasing function of d (every rounded operation is
+// monotone), so equal first and last slots mean every slot is equal.  The
+// arithmetic of both slots is fold_slots' own.
+template <int GEOM, bool GUARD>
+__device__ __forceinline__ void fold_ends(const double (&d)[kR], bool sorted, double P, double IP,
+                                          double ibd, int NB, unsigned& e0, bool& uni) {
+    const double m0 = d[0] * IP, m7 = d[kR - 1] * IP;
+    const double k0 = floor_magic(m0);
+    unsigned a, b;
+    if (GEOM == ATB_GEOM_BINNED) {
+        const int s0 = trunc1_magic(fma(-P, k0, d[0]) * ibd);
+        const int s7 = trunc1_magic(fma(-P, k0, d[kR - 1]) * ibd);
+        a = GUARD ? min((unsigned)s0, (unsigned)NB) : (unsigned)min(max(s0, 1), NB);
+        b = GUARD ? min((unsigned)s7, (unsigned)NB) : (unsigned)min(max(s7, 1), NB);
+    } else {
+        const double nbd = (double)NB;
+        a = min((unsigned)trunc1_magic((m0 - k0) * nbd), (unsigned)NB + 1u);
+        b = min((unsigned)trunc1_magic((m7 - k0) * nbd), (unsigned)NB + 1u);
+    }
+    e0 = a;
+    uni = sorted && m7 < k0 + 1.0 && a == b;
+}
+
+// Fold every staged point of the curve into the group's histograms, each
+// period in its fold mode (kFold*; bin-range passes and global histograms
+// always fold point by point).
 // WIN: bin-range pass -- only slots lo .. lo+W-1 are kept, at entries
 // 0 .. W-1 of H (one period at offset 0).
+// G: the number of the group's periods to fold (its first G).
 template <int GEOM, bool GLOB, int MODE, bool WIN = false>
 __device__ void fold_group(const SearchArgs& a, const GroupSmem& gs, uint4* H, long long so,
-                           long long n_pad, const CurveStat& st, int lo = 0, unsigned W = 0) {
-    const int G = gs.G;
+                           long long n_pad, const CurveStat& st, int G, int lo = 0,
+                           unsigned W = 0) {
     const bool safe = gs.safe_floor != 0;
-    const int L = st.lobits;
+    // split position of the layout's words (count layout for kPackCountT)
+    const int L = MODE == kPackCountT ? curve_lobits(st.n_cnt) : st.lobits;
     const unsigned lomask = (1u << L) - 1u;
     for (long long base = 0; base < n_pad; base += (long long)kBlock * kR) {
         const long long i0 = base + (long long)threadIdx.x * kR;
@@ -793,6 +903,15 @@ __device__ void fold_group(const SearchArgs& a, const GroupSmem& gs, uint4* H, l
                 wb[j] = 0u;
                 wc[j] = (unsigned)qy[j];
                 wd[j] = 0u;
+            } else if (MODE == kPackCountT) {
+                // staged tight words x = count << csh | (q mod 2^lob), z = q >> lob
+                const unsigned x = (unsigned)qw[j];
+                const int q = qy[j] * (1 << st.stage_lob) +
+                              (int)(x & ((1u << st.stage_lob) - 1u));
+                wa[j] = x >> st.stage_csh;
+                wb[j] = 0u;
+                wc[j] = (unsigned)q & lomask;
+                wd[j] = (unsigned)(q >> L);
             } else {
                 wa[j] = MODE == kPackCount ? (unsigned)qw[j] : ((unsigned)qw[j] & lomask);
                 wb[j] = MODE == kPackCount ? 0u : (unsigned)(qw[j] >> L);
@@ -803,11 +922,30 @@ __device__ void fold_group(const SearchArgs& a, const GroupSmem& gs, uint4* H, l
         for (int g = 0; g < G; ++g) {
             const double2 pip = gs.PIP[g];
             const int2 nbb = gs.NBB[g];
+            uint4* H0 = H + nbb.y;
+            const unsigned base0 = GLOB ? 0u : (unsigned)__cvta_generic_to_shared(H0);
+            if (!GLOB && !WIN) {
+                const int fm = gs.fmode[g];  // the same for every lane
+                if (fm != kFoldPoint) {
+                    unsigned e0;
+                    bool uni;
+                    fold_ends<GEOM, GEOM == ATB_GEOM_BINNED>(d, sorted, pip.x, pip.y,
+                                                              st.inv_bin_dur, nbb.x, e0, uni);
+                    unsigned sa = 0u, sb = 0u, sc = 0u, sd = 0u;
+#pragma unroll
+                    for (int j = 0; j < kR; ++j) {
+                        sa += wa[j];
+                        sb += wb[j];
+                        sc += wc[j];
+                        sd += wd[j];
+                    }
+                    if (uni) hist_add_point<false, MODE>(base0, H0, e0, sa, sb, sc, sd);
+                    if (uni) continue;
+                }
+            }
             unsigned e[kR];
             fold_slots<GEOM, GEOM == ATB_GEOM_BINNED && !WIN>(d, sorted, safe, pip.x, pip.y,
                                                              st.inv_bin_dur, nbb.x, e);
-            uint4* H0 = H + nbb.y;
-            const unsigned base0 = GLOB ? 0u : (unsigned)__cvta_generic_to_shared(H0);
 #pragma unroll
             for (int j = 0; j < kR; ++j) {
                 if (WIN) {
@@ -849,9 +987,10 @@ __device__ void window_stats(double dw, double dy, double wtot, double ytot, int
 // Exact sums (W, Y) of raw histogram entry i in layout MODE: the words the
 // layout uses are read directly (component c of entry i is word c ^ rot(i),
 // at byte offset 4c ^ ((i >> 1) & 12) in the entry).
+// `lob` is the split position of the count and split layouts' words.
 template <int MODE>
 __device__ __forceinline__ void entry_sums_m(const longlong2* E, int i, const CurveStat& st,
-                                             long long& w, long long& y) {
+                                             int lob, long long& w, long long& y) {
     const unsigned* ent = reinterpret_cast<const unsigned*>(E + i);
     const unsigned r = slot_rot(i);
     const unsigned x = ent[0u ^ r];
@@ -862,8 +1001,8 @@ __device__ __forceinline__ void entry_sums_m(const longlong2* E, int i, const Cu
     } else {
         const unsigned z = ent[2u ^ r], v = ent[3u ^ r];
         w = MODE == kPackCount ? (long long)x
-                               : (long long)ent[1u ^ r] * (1LL << st.lobits) + (long long)x;
-        y = (long long)(int)v * (1LL << st.lobits) + (long long)z;
+                               : (long long)ent[1u ^ r] * (1LL << lob) + (long long)x;
+        y = (long long)(int)v * (1LL << lob) + (long long)z;
     }
     if (MODE != kPackSplit && !st.cnt_win) w *= (long long)st.qw0;
 }
@@ -872,12 +1011,12 @@ __device__ __forceinline__ void entry_sums_m(const longlong2* E, int i, const Cu
 // their exact int64 sums back in place, return the segment's totals.
 template <int MODE>
 __device__ __forceinline__ void scan_decode(longlong2* E, int b, int e, const CurveStat& st,
-                                            long long& sw, long long& sy) {
+                                            int lob, long long& sw, long long& sy) {
     sw = 0;
     sy = 0;
     for (int i = b; i < e; ++i) {
         long long w, y;
-        entry_sums_m<MODE>(E, i, st, w, y);
+        entry_sums_m<MODE>(E, i, st, lob, w, y);
         E[i] = make_longlong2(w, y);
         sw += w;
         sy += y;
@@ -894,20 +1033,23 @@ __device__ __forceinline__ void scan_decode(longlong2* E, int b, int e, const Cu
 // warp touches in one step fall in distinct bank groups.
 // cw0, cy0: exact sums added to every prefix (the bins below E[0]); the
 // thread holding entry carry_idx stores that entry's exact prefix in *carry.
+// cview: a checked tight curve folded in the count layout (kPackCountT).
 __device__ void team_scan(const Team& tm, GroupSmem& gs, longlong2* E, int M, const CurveStat& st,
-                          long long cw0 = 0, long long cy0 = 0, int carry_idx = -1,
+                          bool cview, long long cw0 = 0, long long cy0 = 0, int carry_idx = -1,
                           longlong2* carry = nullptr) {
     int seg = (M + tm.nthreads - 1) / tm.nthreads;
     seg |= 1;
     const int b = min(M, tm.tid * seg);
     const int e = min(M, b + seg);
     long long sw, sy;
-    if (st.packmode == kPackTight)
-        scan_decode<kPackTight>(E, b, e, st, sw, sy);
+    if (cview)
+        scan_decode<kPackCount>(E, b, e, st, curve_lobits(st.n_cnt), sw, sy);
+    else if (st.packmode == kPackTight)
+        scan_decode<kPackTight>(E, b, e, st, st.lobits, sw, sy);
     else if (st.packmode == kPackCount)
-        scan_decode<kPackCount>(E, b, e, st, sw, sy);
+        scan_decode<kPackCount>(E, b, e, st, st.lobits, sw, sy);
     else
-        scan_decode<kPackSplit>(E, b, e, st, sw, sy);
+        scan_decode<kPackSplit>(E, b, e, st, st.lobits, sw, sy);
     const int lane = threadIdx.x & 31;
     long long iw = sw, iy = sy;
 #pragma unroll
@@ -1226,11 +1368,37 @@ __device__ Cand window_search(const longlong2* E, int NB, int nd, const int* len
 
 template <int GEOM>
 __device__ void finalize_period(const SearchArgs& a, GroupSmem& gs, const Team& tm, longlong2* H,
-                                int g, const CurveStat& st, int nd) {
+                                int g, const CurveStat& st, int nd, bool cview) {
     longlong2* E = H + gs.NBB[g].y;
     const int NB = gs.NBB[g].x;
     const double P = gs.PIP[g].x;
     const double IP = gs.PIP[g].y;
+
+    if (st.tcheck && !cview) {
+        // checked tight layout: the decoded counts of the raw entries (every
+        // slot the fold can write) must add up to the curve's n points, else
+        // a count field overflowed and the period is folded again
+        const int n_ent = (GEOM == ATB_GEOM_BINNED) ? NB + 1 : NB + 2;
+        unsigned cnt = 0u;
+        for (int i = tm.tid; i < n_ent; i += tm.nthreads) {
+            const unsigned* ent = reinterpret_cast<const unsigned*>(E + i);
+            cnt += ent[slot_rot(i)] >> st.cshift;  // component 0 of entry i
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, off);
+        if (tm.nwarps > 1) {
+            const int wg = threadIdx.x >> 5;
+            if ((threadIdx.x & 31) == 0) gs.scan[wg].x = (long long)cnt;
+            team_sync(tm);
+            cnt = 0u;
+            for (int k = 0; k < tm.nwarps; ++k) cnt += (unsigned)gs.scan[tm.warp0 + k].x;
+            team_sync(tm);  // before the scan reuses gs.scan
+        }
+        if (cnt != (unsigned)st.n_cnt) {
+            if (tm.tid == 0) gs.redo[g] = 1;
+            return;  // every thread of the team returns: the same total
+        }
+    }
 
     if (GEOM == ATB_GEOM_BINNED) {
         // padding copy, vbls_v42_parity.cu:78-80: bins 1..os onto NB-os..NB-1
@@ -1265,7 +1433,7 @@ __device__ void finalize_period(const SearchArgs& a, GroupSmem& gs, const Team& 
             gs.L[tm.id][tm.tid] = L;
         }
     }
-    team_scan(tm, gs, E, NB + 1, st);
+    team_scan(tm, gs, E, NB + 1, st, cview);
 
     // scaled exact totals; counting curves: N points of weight qw0s each
     const bool cnt = st.cnt_win != 0;
@@ -1375,6 +1543,8 @@ __device__ void finalize_period(const SearchArgs& a, GroupSmem& gs, const Team& 
 __device__ void run_period_binned_passes(const SearchArgs& a, GroupSmem& gs, longlong2* H,
                                          const CurveStat& st, long long so, long long n_pad,
                                          int nd) {
+    // a checked tight curve is folded here in the count layout (no check)
+    const bool cview = st.tcheck != 0;
     const int NB = gs.NBB[0].x;
     const double P = gs.PIP[0].x;
     const int os = a.oversample;
@@ -1411,12 +1581,14 @@ __device__ void run_period_binned_passes(const SearchArgs& a, GroupSmem& gs, lon
     for (int lo = 0; lo < NB; lo += S) {
         for (int i = threadIdx.x; i < W; i += kBlock) H[i] = make_longlong2(0, 0);
         __syncthreads();
-        if (st.packmode == kPackTight)
-            fold_group<ATB_GEOM_BINNED, false, kPackTight, true>(a, gs, HU, so, n_pad, st, lo, W);
+        if (cview)
+            fold_group<ATB_GEOM_BINNED, false, kPackCountT, true>(a, gs, HU, so, n_pad, st, 1, lo, W);
+        else if (st.packmode == kPackTight)
+            fold_group<ATB_GEOM_BINNED, false, kPackTight, true>(a, gs, HU, so, n_pad, st, 1, lo, W);
         else if (st.packmode == kPackCount)
-            fold_group<ATB_GEOM_BINNED, false, kPackCount, true>(a, gs, HU, so, n_pad, st, lo, W);
+            fold_group<ATB_GEOM_BINNED, false, kPackCount, true>(a, gs, HU, so, n_pad, st, 1, lo, W);
         else
-            fold_group<ATB_GEOM_BINNED, false, kPackSplit, true>(a, gs, HU, so, n_pad, st, lo, W);
+            fold_group<ATB_GEOM_BINNED, false, kPackSplit, true>(a, gs, HU, so, n_pad, st, 1, lo, W);
         __syncthreads();
         // padding copy, vbls_v42_parity.cu:78-80: bins 1..os (saved by the
         // first pass) replace bins NB-os..NB-1 wherever a pass holds them
@@ -1430,7 +1602,7 @@ __device__ void run_period_binned_passes(const SearchArgs& a, GroupSmem& gs, lon
         const int M = min(W, NB + 1 - lo);
         const longlong2 c0 = gs.carry;
         __syncthreads();
-        team_scan(tm, gs, H, M, st, c0.x, c0.y, S - 1 < M ? S - 1 : -1, &gs.carry);
+        team_scan(tm, gs, H, M, st, cview, c0.x, c0.y, S - 1 < M ? S - 1 : -1, &gs.carry);
         Cand best{-1.0f, 1.0f, 0x7fffffff};
         if (wtot > 0.0) {
             const WinRange rg{lo, lo, min(lo + S, NB), min(NB, lo + W - 1)};
@@ -1500,21 +1672,10 @@ __device__ void run_period_binned_passes(const SearchArgs& a, GroupSmem& gs, lon
     __syncthreads();
 }
 
-template <int GEOM, bool GLOB>
-__device__ void run_group(const SearchArgs& a, GroupSmem& gs, longlong2* H, const CurveStat& st,
-                          long long so, long long n_pad, int nd) {
-    const int total = gs.total;
-    for (int i = threadIdx.x; i < total; i += kBlock) H[i] = make_longlong2(0, 0);
-    __syncthreads();
-    uint4* HU = reinterpret_cast<uint4*>(H);
-    if (st.packmode == kPackTight)
-        fold_group<GEOM, GLOB, kPackTight>(a, gs, HU, so, n_pad, st);
-    else if (st.packmode == kPackCount)
-        fold_group<GEOM, GLOB, kPackCount>(a, gs, HU, so, n_pad, st);
-    else
-        fold_group<GEOM, GLOB, kPackSplit>(a, gs, HU, so, n_pad, st);
-    __syncthreads();
-    const int G = gs.G;
+// Teams of warps finalise the group's first G periods.
+template <int GEOM>
+__device__ void finalize_group(const SearchArgs& a, GroupSmem& gs, longlong2* H,
+                               const CurveStat& st, int nd, int G, bool cview) {
     // teams of tw warps (a power of two; teams as wide as 1/G of the CTA
     // measured slower); multi-warp teams synchronise on named barriers 1..15,
     // so at most 15 of them may exist
@@ -1529,8 +1690,61 @@ __device__ void run_group(const SearchArgs& a, GroupSmem& gs, longlong2* H, cons
     tm.nthreads = tw * 32;
     tm.warp0 = tm.id * tw;
     tm.tid = threadIdx.x - tm.warp0 * 32;
-    for (int g = tm.id; g < G; g += n_teams) finalize_period<GEOM>(a, gs, tm, H, g, st, nd);
+    for (int g = tm.id; g < G; g += n_teams) finalize_period<GEOM>(a, gs, tm, H, g, st, nd, cview);
     __syncthreads();
+}
+
+template <int GEOM, bool GLOB>
+__device__ void run_group(const SearchArgs& a, GroupSmem& gs, longlong2* H, const CurveStat& st,
+                          long long so, long long n_pad, int nd) {
+    const int total = gs.total;
+    for (int i = threadIdx.x; i < total; i += kBlock) H[i] = make_longlong2(0, 0);
+    __syncthreads();
+    uint4* HU = reinterpret_cast<uint4*>(H);
+    // global histograms fold a checked tight curve in the count layout at once
+    const bool cview = GLOB && st.tcheck;
+    const int G = gs.G;
+    if (cview)
+        fold_group<GEOM, GLOB, kPackCountT>(a, gs, HU, so, n_pad, st, G);
+    else if (st.packmode == kPackTight)
+        fold_group<GEOM, GLOB, kPackTight>(a, gs, HU, so, n_pad, st, G);
+    else if (st.packmode == kPackCount)
+        fold_group<GEOM, GLOB, kPackCount>(a, gs, HU, so, n_pad, st, G);
+    else
+        fold_group<GEOM, GLOB, kPackSplit>(a, gs, HU, so, n_pad, st, G);
+    __syncthreads();
+    finalize_group<GEOM>(a, gs, H, st, nd, G, cview);
+    if (!GLOB && st.tcheck) {
+        // periods whose counts overflowed the tight words: fold them again in
+        // the count layout (their entries only) and finalise them.  The
+        // group's arrays are compacted to those periods (only the first r
+        // are used from here on; the caller advances by G, which no thread
+        // writes here).
+        if (threadIdx.x == 0) {
+            int r = 0;
+            for (int k = 0; k < G; ++k) {
+                if (!gs.redo[k]) continue;
+                gs.PIP[r] = gs.PIP[k];
+                gs.NBB[r] = gs.NBB[k];
+                gs.slot[r] = gs.slot[k];
+                gs.fmode[r] = gs.fmode[k];
+                ++r;
+            }
+            gs.n_redo = r;
+        }
+        __syncthreads();
+        const int r = gs.n_redo;
+        if (r > 0) {
+            for (int k = 0; k < r; ++k) {
+                const int off = gs.NBB[k].y, cnt = gs.NBB[k].x + 2;
+                for (int i = threadIdx.x; i < cnt; i += kBlock) H[off + i] = make_longlong2(0, 0);
+            }
+            __syncthreads();
+            fold_group<GEOM, false, kPackCountT>(a, gs, HU, so, n_pad, st, r);
+            __syncthreads();
+            finalize_group<GEOM>(a, gs, H, st, nd, r, true);
+        }
+    }
 }
 
 template <int GEOM>
@@ -1617,6 +1831,17 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) search_kernel(const Search
                 }
                 gs.safe_floor =
                     fold_safe<GEOM>(st.dt_absmax * ipmax, pmax * st.inv_bin_dur) ? 1 : 0;
+                // fold mode per period: expected time-ordered points per bin
+                // (the plain staged order holds consecutive points per lane)
+                const bool dense_ok = gs.safe_floor && !gs.glob && !st.ilv;
+                for (int k = 0; k < g; ++k) {
+                    const double bw = (GEOM == ATB_GEOM_BINNED)
+                                          ? st.bin_dur
+                                          : gs.PIP[k].x / (double)gs.NBB[k].x;
+                    const double run = bw * st.density;
+                    gs.fmode[k] = dense_ok && run >= a.merge_run ? kFoldChunk : kFoldPoint;
+                    gs.redo[k] = 0;
+                }
             }
             __syncthreads();
             if (gs.glob == 2) {
@@ -1972,6 +2197,11 @@ cudaError_t plan_read(atb_plan* p, void* dst, const void* src, size_t bytes) {
     return e == cudaSuccess ? cudaStreamSynchronize(p->stream) : e;
 }
 
+// Fold-mode threshold from its atb_params field: 0 = the default, < 0 = never.
+double fold_threshold(int32_t v, double dflt) {
+    return v == 0 ? dflt : (v < 0 ? 1.0e300 : (double)v);
+}
+
 int launch_stage(atb_plan* p, cudaStream_t s) {
     if (p->y_is_f64)
         stage_kernel<double><<<p->n_curves, kStageBlock, 0, s>>>(p->sa);
@@ -2308,6 +2538,7 @@ int plan_create(atb_handle* h, const atb_params* prm, const atb_batch* b, const 
     qa.power = o->power;
     qa.best_key = reinterpret_cast<unsigned long long*>(o->best_key);
     qa.tile_p = tile_p;
+    qa.merge_run = fold_threshold(prm->merge_run, kDefaultMergeRun);
     qa.depth = o->depth;
     qa.depth_err = o->depth_err;
     qa.t0 = o->t0;
@@ -2364,7 +2595,7 @@ int atb_plan_curve_layout(atb_plan* p, int32_t* layout, int32_t* occupancy_bits)
     std::vector<CurveStat> st(p->n_curves);
     ATB_CUDA(p->h, plan_read(p, st.data(), p->sa.stats, sizeof(CurveStat) * st.size()));
     for (int c = 0; c < p->n_curves; ++c) {
-        layout[c] = st[c].packmode;
+        layout[c] = st[c].tcheck ? ATB_LAYOUT_TIGHT_CHECKED : st[c].packmode;
         occupancy_bits[c] = st[c].occ_bits;
     }
     return ATB_OK;
@@ -2860,6 +3091,7 @@ extern "C" int atb_search_curve_static(const atb_params* prm, const double* t, c
     qa.ghist_stride = 0;
     qa.tile_counter = &m->tile_counter;
     qa.tile_p = kTileP;
+    qa.merge_run = fold_threshold(prm->merge_run, kDefaultMergeRun);
     qa.status = &m->status;
     int occ = 1;
     if (prm->geometry == ATB_GEOM_BINNED)

@@ -12,7 +12,7 @@ sm_100a kernels of ``libastrotransit_b200.so``.
 from __future__ import annotations
 
 import ctypes
-from dataclasses import dataclass, field
+from dataclasses import dataclass, field, replace
 from typing import Dict, List, Optional, Sequence
 
 import numpy as np
@@ -34,6 +34,10 @@ class SearchConfig:
     tile_periods  periods per work-queue tile (1..64); 0 = chosen from the
                batch size, or the value BLSEngine.autotune found for this
                kind of batch.  Results never depend on it.
+    merge_run  fold strategy: expected time-ordered points per bin from
+               which a thread adds the points it holds once when they share a
+               slot (0 = the default 8, or the value the autotuner found;
+               < 0 = never).  Results never depend on it.
     """
     method: str = "parity"
     objective: Optional[str] = None
@@ -41,6 +45,7 @@ class SearchConfig:
     oversample: int = 10
     max_bins: Optional[int] = None
     tile_periods: int = 0
+    merge_run: int = 0
 
     def params(self) -> N.Params:
         if self.method == "fast":
@@ -48,14 +53,15 @@ class SearchConfig:
             if obj != "fast":
                 raise ValueError("method='fast' uses the reference's fast score")
             return N.Params(N.GEOM_FIXED, N.OBJ_FAST, int(self.n_bins), int(self.oversample), 0,
-                            int(self.tile_periods))
+                            int(self.tile_periods), int(self.merge_run), 0)
         if self.method == "parity":
             obj = self.objective or "snr"
             if obj not in ("snr", "likelihood"):
                 raise ValueError("method='parity' supports objective 'snr' or 'likelihood'")
             mb = 0 if self.max_bins is None else int(self.max_bins)
             return N.Params(N.GEOM_BINNED, N.OBJECTIVES[obj], int(self.n_bins),
-                            int(self.oversample), mb, int(self.tile_periods))
+                            int(self.oversample), mb, int(self.tile_periods),
+                            int(self.merge_run), 0)
         raise ValueError(f"unknown method {self.method!r} (expected 'fast' or 'parity')")
 
 
@@ -272,8 +278,8 @@ class SearchPlan:
 
     def curve_layout(self):
         """After an execution: (layout, occupancy_bits) per curve, numpy int32.
-        layout is ATB_LAYOUT_SPLIT / COUNT / TIGHT (0 / 1 / 2), the histogram
-        word layout the search used; occupancy_bits is the bit length of the
+        layout is ATB_LAYOUT_SPLIT / COUNT / TIGHT / TIGHT_CHECKED (0 / 1 / 2 /
+        3), the histogram word layout the search used; occupancy_bits is the bit length of the
         curve's bound on points per bin (64: no bound).  Synchronous."""
         nc = self.batch.n_curves
         lay = np.zeros(nc, np.int32)
@@ -319,7 +325,7 @@ class BLSEngine:
         # device, persisted across processes
         self.tuning = TuningTable(table_path(name, torch.cuda.get_device_capability(dev)), name,
                                   self.handle.lib.atb_version().decode()).load()
-        self.last_tune: Dict[int, float] = {}
+        self.last_tune: Dict[str, float] = {}
 
     @classmethod
     def get(cls, device=None) -> "BLSEngine":
@@ -369,46 +375,68 @@ class BLSEngine:
         b = lambda v: int(np.log2(max(v, 1.0)))  # noqa: E731
         return (config.method, b(nc), b(pts), b(per))
 
+    # fold strategies the autotuner tries (merge_run)
+    FOLD_CANDIDATES = (0, -1, 4, 16)
+
+    def _time_search(self, batch: CurveBatch, cfg: SearchConfig, repeats: int) -> float:
+        plan = SearchPlan(self, batch, cfg, self.allocate_outputs(batch))
+        try:
+            plan.execute()
+            torch.cuda.synchronize(batch.device)
+            return min(plan.profile()["search"] for _ in range(max(1, repeats)))
+        finally:
+            plan.close()
+
     def autotune(self, batch: CurveBatch, config: SearchConfig,
-                 candidates: Sequence[int] = (8, 16, 32, 64), repeats: int = 2,
-                 persist: bool = True) -> int:
-        """Time the search kernel on `batch` for each tile size in `candidates`
-        (results are identical for all), keep the fastest for this kind of
-        batch (``tune_key``) in the engine's tuning table -- written to its
-        file unless `persist` is false -- and return it; later plans with
-        ``tile_periods == 0`` use it, in this process and in later ones."""
-        times = {}
+                 candidates: Sequence[int] = (8, 16, 32, 64),
+                 fold_candidates: Sequence[tuple] = FOLD_CANDIDATES, repeats: int = 2,
+                 persist: bool = True) -> Dict[str, int]:
+        """Time the search kernel on `batch` over the knobs that never change
+        a result -- first the tile sizes in `candidates` (periods per
+        work-queue tile), then, at the fastest of those, the fold strategies
+        in `fold_candidates` (merge_run values) -- keep the
+        fastest setting for this kind of batch (``tune_key``) in the engine's
+        tuning table, written to its file unless `persist` is false, and
+        return it.  Later plans whose config leaves a knob at 0 use the tuned
+        value, in this process and in later ones."""
+        times: Dict[str, float] = {}
+        best_tp, best_ms = None, None
         for tp in candidates:
-            cfg = SearchConfig(config.method, config.objective, config.n_bins, config.oversample,
-                               config.max_bins, int(tp))
-            plan = SearchPlan(self, batch, cfg, self.allocate_outputs(batch))
-            try:
-                plan.execute()
-                torch.cuda.synchronize(batch.device)
-                times[int(tp)] = min(plan.profile()["search"] for _ in range(max(1, repeats)))
-            finally:
-                plan.close()
-        best = min(times, key=times.get)
+            ms = self._time_search(batch, replace(config, tile_periods=int(tp)), repeats)
+            times[f"tile={int(tp)}"] = ms
+            if best_ms is None or ms < best_ms:
+                best_tp, best_ms = int(tp), ms
+        best_fold = int(config.merge_run)
+        for mr in fold_candidates:
+            cfg = replace(config, tile_periods=best_tp, merge_run=int(mr))
+            ms = self._time_search(batch, cfg, repeats)
+            times[f"tile={best_tp},merge_run={mr}"] = ms
+            if ms < best_ms:
+                best_fold, best_ms = int(mr), ms
+        settings = {"tile_periods": best_tp, "merge_run": best_fold}
         self.tuning.put(self.tune_key(batch, config),
-                        {"tile_periods": int(best),
-                         "search_ms": {str(k): float(v) for k, v in times.items()}})
+                        {**settings, "search_ms": times, "best_ms": best_ms})
         if persist:
             self.tuning.save()
         self.last_tune = times
-        return best
+        return settings
+
+    def tuned_config(self, batch: CurveBatch, config: SearchConfig) -> SearchConfig:
+        """`config` with every knob it leaves at 0 set from the tuning table
+        (when this kind of batch has been tuned)."""
+        tuned = self.tuning.get(self.tune_key(batch, config))
+        if not tuned:
+            return config
+        upd = {k: int(tuned[k]) for k in ("tile_periods", "merge_run")
+               if k in tuned and getattr(config, k) == 0}
+        return replace(config, **upd) if upd else config
 
     def plan(self, batch: CurveBatch, config: SearchConfig,
              outputs: Optional[Dict[str, torch.Tensor]] = None,
              stream: Optional[torch.cuda.Stream] = None) -> SearchPlan:
         if outputs is None:
             outputs = self.allocate_outputs(batch)
-        if config.tile_periods == 0:
-            tuned = self.tuning.get(self.tune_key(batch, config))
-            if tuned is not None and "tile_periods" in tuned:
-                config = SearchConfig(config.method, config.objective, config.n_bins,
-                                      config.oversample, config.max_bins,
-                                      int(tuned["tile_periods"]))
-        return SearchPlan(self, batch, config, outputs, stream)
+        return SearchPlan(self, batch, self.tuned_config(batch, config), outputs, stream)
 
     def screen(self, batch: CurveBatch, config: SearchConfig,
                stream: Optional[torch.cuda.Stream] = None) -> Dict[str, torch.Tensor]:

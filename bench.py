@@ -61,8 +61,8 @@ OVERSAMPLE = 10
 E2E_PARTS = 8  # runs of curves (and streams) of the end-to-end step
 # 32-bit shared-memory reductions per (point, period) fold update, by the
 # histogram word layout the stage kernel chose for the curve
-LAYOUT_WORDS = {0: 4, 1: 3, 2: 2}  # split, count, tight
-LAYOUT_NAMES = {0: "split", 1: "count", 2: "tight"}
+LAYOUT_WORDS = {0: 4, 1: 3, 2: 2, 3: 2}  # split, count, tight, tight (checked)
+LAYOUT_NAMES = {0: "split", 1: "count", 2: "tight", 3: "tight_checked"}
 U64_BYTES_PER_FOLD = 16  # two 8-byte accumulations per update in a 64-bit design
 
 
@@ -339,33 +339,39 @@ def plain_gpu_baseline(wl, budget_s, device):
 
 # ---------------------------------------------------------------- serving ---
 
-def serving_requests(rate, seconds, seed=4000):
+SERVING_POOL = 2000  # distinct request curves; longer runs draw from them
+
+
+def serving_pool(n, seed=4000):
+    """`n` request curves of the uneven-batch distribution (fast method,
+    4-8 durations each)."""
     import recipes as R
     rng = np.random.default_rng(seed)
-    n_req = max(1, int(rate * seconds))
-    reqs = []
-    for _ in range(n_req):
-        n_sec, cad, n, n_per = R.mixed_curve_spec(rng)
-        t, y, dy, per = R.mixed_curve(rng, n_sec, cad, n, n_per)
-        reqs.append(dict(t=t, y=y, dy=dy, periods=per,
+    pool = []
+    for _ in range(n):
+        n_sec, cad, npts, n_per = R.mixed_curve_spec(rng)
+        t, y, dy, per = R.mixed_curve(rng, n_sec, cad, npts, n_per)
+        pool.append(dict(t=t, y=y, dy=dy, periods=per,
                          durations=R.C2_DURATIONS[:4 + int(rng.integers(0, 5))], method="fast"))
-    gaps = rng.exponential(1.0 / rate, n_req)
-    return reqs, gaps
+    return pool
 
 
-def run_serving(device, rate, seconds, per_call_loop=False):
-    """Continuous-batching server under Poisson arrivals: each request is one
-    curve of the uneven-batch distribution (fast method, 4-8 durations);
-    returns p50/p99 latency from submission to result and the completed rate,
-    and optionally the rate of a one-call-per-curve loop over the same
-    requests (BoxLeastSquaresGPU.power, back to back)."""
+def run_serving(device, rate, seconds, pool, seed=4001):
+    """Continuous-batching server under Poisson arrivals at `rate` requests/s
+    for `seconds`: each request is a curve drawn from `pool`; returns p50/p99
+    latency from submission to result and the completed rate."""
     from astro_transit_gpu_b200.serving import BLSServer
-    reqs, gaps = serving_requests(rate, seconds)
+    rng = np.random.default_rng(seed)
+    n_req = max(1, int(rate * seconds))
+    # distinct curves while the pool lasts, then draws with replacement
+    picks = (rng.permutation(len(pool))[:n_req] if n_req <= len(pool)
+             else rng.integers(0, len(pool), n_req))
+    gaps = rng.exponential(1.0 / rate, n_req)
     with BLSServer(device=device, memory_budget=120e9, max_batch=512, n_streams=2) as srv:
         # warm-up (library load, allocator pools at the sizes of large
         # batches): one request, then a burst of 64 at once; not timed
-        srv.submit(**reqs[0]).result(timeout=300)
-        for f in [srv.submit(**r) for r in reqs[:64]]:
+        srv.submit(**pool[0]).result(timeout=300)
+        for f in [srv.submit(**r) for r in pool[:64]]:
             f.result(timeout=300)
         srv.reset_stats()
         # the objects alive now (this process's workload arrays) are not
@@ -376,41 +382,44 @@ def run_serving(device, rate, seconds, per_call_loop=False):
             t0 = time.perf_counter()
             due = t0 + np.cumsum(gaps)
             futs = []
-            for r, d in zip(reqs, due):
+            for i, d in zip(picks, due):
                 wait = d - time.perf_counter()
                 if wait > 0:
                     time.sleep(wait)
-                futs.append(srv.submit(**r))
+                futs.append(srv.submit(**pool[int(i)]))
             for f in futs:
-                f.result(timeout=600)
+                f.result(timeout=3600)
             wall = time.perf_counter() - t0
         finally:
             gc.unfreeze()
         st = srv.stats()
-    out = {"arrivals": "Poisson", "offered_rate_per_s": rate, "requests": len(reqs),
-           "seconds": seconds, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
-           "mean_ms": st["mean_ms"], "completed_curves_per_s": st["curves_per_s"],
-           "wall_s": wall, "batches": st["batches"],
-           "request": "one uneven-batch curve (N log-U[1e3, 2e5], 1-13 sectors, 1000-60000 "
-                      "periods), fast method, 4-8 durations 0.02-0.30 d",
-           "admission": "120 GB device-memory budget, up to 512 requests per batch, "
-                        "2 batches in flight"}
-    if per_call_loop:
-        import torch
-        from astro_transit_gpu_b200.api import BoxLeastSquaresGPU
-        r0 = reqs[0]
-        BoxLeastSquaresGPU(r0["t"], r0["y"], r0["dy"]).power(r0["periods"], r0["durations"])
-        torch.cuda.synchronize(device)
-        t0 = time.perf_counter()
-        for r in reqs:
-            BoxLeastSquaresGPU(r["t"], r["y"], r["dy"]).power(r["periods"], r["durations"],
-                                                              method="fast")
-        loop_s = time.perf_counter() - t0
-        out["per_call_loop_curves_per_s"] = len(reqs) / loop_s
-        out["per_call_loop"] = ("one BoxLeastSquaresGPU.power call per request, back to back "
-                                "(no arrival pacing): the plain one-call-per-curve path's "
-                                "largest sustainable rate")
-    return out
+    return {"arrivals": "Poisson", "offered_rate_per_s": rate, "requests": n_req,
+            "seconds": seconds, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+            "mean_ms": st["mean_ms"], "completed_curves_per_s": st["curves_per_s"],
+            "wall_s": wall, "batches": st["batches"],
+            "request": f"a curve drawn from {len(pool)} of the uneven-batch distribution "
+                       "(N log-U[1e3, 2e5], 1-13 sectors, 1000-60000 periods), fast method, "
+                       "4-8 durations 0.02-0.30 d",
+            "admission": "120 GB device-memory budget, up to 512 requests per batch, "
+                         "2 batches in flight"}
+
+
+def per_call_rate(device, pool, n=500):
+    """Curves/s of the plain one-call-per-curve path on the same requests: one
+    BoxLeastSquaresGPU.power call per curve, back to back (no arrival pacing),
+    i.e. the largest rate that path sustains."""
+    import torch
+    from astro_transit_gpu_b200.api import BoxLeastSquaresGPU
+    r0 = pool[0]
+    BoxLeastSquaresGPU(r0["t"], r0["y"], r0["dy"]).power(r0["periods"], r0["durations"])
+    torch.cuda.synchronize(device)
+    reqs = pool[:min(n, len(pool))]
+    t0 = time.perf_counter()
+    for r in reqs:
+        BoxLeastSquaresGPU(r["t"], r["y"], r["dy"]).power(r["periods"], r["durations"],
+                                                          method="fast")
+    return {"curves_per_s": len(reqs) / (time.perf_counter() - t0), "requests": len(reqs),
+            "path": "one BoxLeastSquaresGPU.power call per request, back to back"}
 
 
 # ------------------------------------------------------------------ arms ---
@@ -554,7 +563,8 @@ def main(argv=None):
     peak = 4.0 * peaks["smem_red_u32_per_s"] / 1e9
     ach64 = U64_BYTES_PER_FOLD * u_fold / (ms_search * 1e-3) / 1e9
     peak64 = 8.0 * peaks["smem_red_u64_per_s"] / 1e9
-    layout_share = {LAYOUT_NAMES[k]: float(upd[layout == k].sum() / u_fold) for k in (0, 1, 2)}
+    layout_share = {LAYOUT_NAMES[k]: float(upd[layout == k].sum() / u_fold)
+                    for k in LAYOUT_NAMES}
 
     total_curves = world * nc * args.steps
     value = total_curves / (ms * 1e-3)
@@ -579,7 +589,8 @@ def main(argv=None):
             else None,
             "units": "4 B per 32-bit shared-memory reduction the fold issues: 2, 3 or 4 per "
                      "(point, period) update by the curve's histogram layout (tight, count, "
-                     f"split); {u_fold:.3e} updates and {red_bytes / 4:.3e} reductions per launch",
+                     f"split; a checked tight period that is folded again counts 2); "
+                     f"{u_fold:.3e} updates and {red_bytes / 4:.3e} reductions per launch",
             "layout_share_of_updates": layout_share,
             "peak_source": "atb_bench_smem_red_u32 (conflict-free 32-bit shared-memory "
                            "reductions, measured live on this GPU)",
@@ -626,11 +637,15 @@ def main(argv=None):
     if world == 1 and not args.no_serving:
         # the server runs alone on the device, as in a serving process, and
         # before the CPU baseline loads every host core
-        line["serving"] = run_serving(dev, args.serving_rate, args.serving_seconds)
-        if args.serving_rates:
-            line["serving_sweep"] = [
-                run_serving(dev, float(r), args.serving_seconds, per_call_loop=True)
-                for r in args.serving_rates.split(",")]
+        rates = ([float(r) for r in args.serving_rates.split(",")] if args.serving_rates
+                 else [])
+        pool = serving_pool(min(SERVING_POOL, max(64, int(max([args.serving_rate] + rates)
+                                                              * args.serving_seconds))))
+        line["serving"] = run_serving(dev, args.serving_rate, args.serving_seconds, pool)
+        if rates:
+            line["serving_sweep"] = {
+                "rates": [run_serving(dev, r, args.serving_seconds, pool) for r in rates],
+                "per_call_path": per_call_rate(dev, pool)}
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload != "precision":
         rate, cores, sample, outs, _ = cpu_reference(wl, args.method, args.cpu_seconds)
         sl = [slice(int(ob[c]), int(ob[c]) + len(o["power"])) for c, o in enumerate(outs)]

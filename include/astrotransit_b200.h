@@ -60,6 +60,13 @@ typedef struct {
                            n_bins = min(n_bins, max_bins-1), vbls_v42_parity.cu:46-47 */
     int32_t tile_periods; /* periods per work-queue tile, 1..64; 0 = chosen from the batch
                              size (no reference counterpart; results do not depend on it) */
+    /* Fold strategy (no reference counterpart; results do not depend on it): a
+     * period whose bins hold at least merge_run time-ordered points on average
+     * (bin width x the curve's mean point density) adds the points a thread
+     * holds once when they provably share a slot.  0 = the default (8),
+     * < 0 = never. */
+    int32_t merge_run;
+    int32_t reserved;   /* must be 0 */
 } atb_params;
 
 /*
@@ -164,12 +171,16 @@ int atb_plan_top_k(atb_plan* p, int32_t k, int32_t distance, int32_t* out_idx, v
  * its bin-occupancy bound (64: no bound).  Layouts: ATB_LAYOUT_SPLIT (weights
  * not uniform), ATB_LAYOUT_COUNT (uniform weights), ATB_LAYOUT_TIGHT (uniform
  * weights and fewer than 2^12 points can share a bin: two 32-bit reductions
- * per point instead of three).  The layout never changes the results.
+ * per point instead of three), ATB_LAYOUT_TIGHT_CHECKED (uniform weights, no
+ * proven bound but few points per bin on average: the two-word layout, with
+ * each period's point count checked and a period whose bin overflowed folded
+ * again in the count layout).  The layout never changes the results.
  * Synchronous; both arrays hold one entry per curve.
  */
 #define ATB_LAYOUT_SPLIT 0
 #define ATB_LAYOUT_COUNT 1
 #define ATB_LAYOUT_TIGHT 2
+#define ATB_LAYOUT_TIGHT_CHECKED 3
 int atb_plan_curve_layout(atb_plan* p, int32_t* layout, int32_t* occupancy_bits);
 
 /* One-shot: create, execute on `stream`, synchronise, check, destroy. */

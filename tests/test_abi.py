@@ -43,7 +43,7 @@ def test_null_handles_are_rejected_without_a_device():
 
 
 def test_structs_match_header_layout():
-    # int32 x6 params; batch: 2 ints + 7 host pointers + 5 device pointers
-    assert ctypes.sizeof(N.Params) == 24
+    # int32 x8 params; batch: 2 ints + 7 host pointers + 5 device pointers
+    assert ctypes.sizeof(N.Params) == 32
     assert ctypes.sizeof(N.Batch) == 8 + 12 * 8
     assert ctypes.sizeof(N.Outputs) == 8 * 8

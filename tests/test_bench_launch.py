@@ -30,7 +30,7 @@ def test_bench_defaults():
     assert a.warmup >= 3
     assert bench.parse(["--workload", "mixed"]).curves == 8192
     assert bench.parse(["--workload", "precision"]).curves == 512
-    assert bench.LAYOUT_WORDS == {0: 4, 1: 3, 2: 2}
+    assert bench.LAYOUT_WORDS == {0: 4, 1: 3, 2: 2, 3: 2}
 
 
 def test_indexed_uneven_batch_is_split_by_lpt_without_overlap():

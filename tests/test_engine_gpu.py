@@ -534,13 +534,16 @@ def test_tile_size_never_changes_results_and_autotune_picks_one(engine, tmp_path
     engine.tuning = TuningTable(str(tmp_path / "tuning.json"), saved.device_name,
                                 saved.library)
     try:
-        best = engine.autotune(b, cfg, candidates=(8, 64))
-        assert best in (8, 64) and set(engine.last_tune) == {8, 64}
+        best = engine.autotune(b, cfg, candidates=(8, 64), fold_candidates=(0, 1, -1))
+        assert best["tile_periods"] in (8, 64)
+        assert best["merge_run"] in (0, 1, -1)
+        assert len(engine.last_tune) == 5
         key = engine.tune_key(b, cfg)
-        assert engine.tuning.get(key)["tile_periods"] == best
+        assert engine.tuning.get(key)["tile_periods"] == best["tile_periods"]
         # persisted: a table read back from the file holds the same setting
         again = TuningTable(engine.tuning.path, saved.device_name, saved.library).load()
-        assert again.get(key)["tile_periods"] == best
+        assert {k: again.get(key)[k] for k in best} == best
+        assert engine.tuned_config(b, cfg).tile_periods == best["tile_periods"]
         # the tuned plan gives what the default plan gave
         out = {k: v.cpu().numpy() for k, v in engine.search(b, cfg).items()}
         for k in ref:

@@ -15,7 +15,7 @@ from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
-SPLIT, COUNT, TIGHT = 0, 1, 2
+SPLIT, COUNT, TIGHT, CHECKED = 0, 1, 2, 3
 FIELDS = ("power", "depth", "depth_err", "t0", "duration", "window")
 
 
@@ -126,16 +126,20 @@ def test_tight_layout_bound_holds_and_results_bit_exact(engine, name):
 
 
 def test_layout_falls_back_when_no_bound(engine):
+    """Without a proven occupancy bound, sparse-on-average uniform curves use
+    the checked tight layout; a cap that the grid reaches, or non-uniform
+    weights, use the count and split layouts."""
     rng = np.random.default_rng(8)
     periods, durs = np.geomspace(0.5, 5.0, 200), np.array([0.05, 0.1])
     # dense: 20000 samples within 0.05 d -> a bound of ~6000 points per bin
     t = np.sort(rng.uniform(0, 0.05, 20000)) + 10.0
     y = 1.0 + rng.normal(0, 1e-3, t.size)
     cases = [
-        (t, y, None, "binned", None, COUNT),
+        (t, y, None, "binned", None, CHECKED),
         # unsorted times: no bound is computed
         (rng.permutation(R.c0_curve(n=4000, seed=4)[0]), rng.normal(1, 1e-3, 4000), None,
-         "binned", None, COUNT),
+         "binned", None, CHECKED),
+        (t, y, None, "fixed", None, CHECKED),
         # a bin cap that the grid reaches folds many points into the last bin
         (*R.c0_curve(n=4000, seed=4)[:2], None, "binned", 500, COUNT),
         # non-uniform weights
@@ -146,8 +150,41 @@ def test_layout_falls_back_when_no_bound(engine):
         cfg = _cfg(kind, max_bins=mb)
         g, lay, bits = run_with_layout(engine, t_, y_, w_, periods, durs, cfg)
         assert lay == expect, (expect, lay, bits)
-        if w_ is None:
+        if w_ is None and expect != CHECKED:
             assert bits == expected_bits(t_, periods, durs, cfg) == 64
         o = oracle_for(t_, y_, w_, periods, durs, cfg)
         for k in FIELDS:
             assert np.array_equal(np.asarray(g[k]), np.asarray(o[k])), (expect, k)
+
+
+@pytest.mark.parametrize("kind", ["binned", "fixed"])
+def test_checked_tight_layout_refolds_overflowing_periods(engine, kind):
+    """12 000 samples within 0.002 d among 8 000 spread over 27 d: at every
+    period more than 2^12 points share one bin, so every period's count check
+    fails and the period is folded again in the count layout; a batch mixing
+    that curve with ordinary ones, and the curve alone, match the oracle bit
+    for bit."""
+    from astro_transit_gpu_b200.engine import CurveBatch, split_outputs
+    rng = np.random.default_rng(12)
+    t = np.sort(np.concatenate([rng.uniform(0, 0.002, 12000),
+                                rng.uniform(0.5, 27.0, 8000)])) + 3000.0
+    y = R.inject_box(t, 1.0 + rng.normal(0, 1e-3, t.size), 2.2, 3000.7, 0.1, 3e-3)
+    y = y.astype(np.float32)
+    periods, durs = np.geomspace(0.5, 10.0, 300), np.array([0.04, 0.08, 0.16])
+    cfg = _cfg(kind, n_bins=200)
+    g, lay, _ = run_with_layout(engine, t, y, None, periods, durs, cfg)
+    assert lay == CHECKED
+    o = oracle_for(t, y, None, periods, durs, cfg)
+    for k in FIELDS:
+        assert np.array_equal(np.asarray(g[k]), np.asarray(o[k])), k
+    assert max_occupancy(engine, t, y, None, periods, durs, cfg) >= 4096
+    # in a batch with curves that pass the check
+    t2, y2 = R.c0_curve(n=9000, seed=13)[:2]
+    b = CurveBatch.from_arrays([t2, t, t2], [y2.astype(np.float32), y, y2.astype(np.float32)],
+                               periods=periods, durations=durs)
+    outs = split_outputs(b, engine.search(b, cfg))
+    o2 = oracle_for(t2, y2, None, periods, durs, cfg)
+    for k in FIELDS:
+        assert np.array_equal(np.asarray(outs[1][k]), np.asarray(o[k])), k
+        assert np.array_equal(np.asarray(outs[0][k]), np.asarray(o2[k])), k
+        assert np.array_equal(np.asarray(outs[2][k]), np.asarray(o2[k])), k
