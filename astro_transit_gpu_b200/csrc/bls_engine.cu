@@ -4,7 +4,7 @@
 // Hot path (one astropy-style BLS per (light curve, period)):
 //   stage kernel   one CTA per curve: t_start = t[0], dt = t - t_start (FP64),
 //                  deterministic fixed-point staging q_w = rint(w*2^s_w),
-//                  q_y = rint(w*(y-c)*2^s_y) (|q| <= 2^26), per-curve totals,
+//                  q_y = rint(w*(y-c)*2^s_y) (|q| <= 2^27), per-curve totals,
 //                  the curve's histogram word layout (kPack*) and staged order.
 //   search kernel  persistent; CTAs pop (curve, period-chunk) tiles from a
 //                  device counter.  Periods of a tile are packed into groups
@@ -81,7 +81,7 @@ constexpr double kMagicFloor = 6755399441055744.0;  // 1.5*2^52: (m + C)(rd) - C
 //               K the most points inside any time window one bin wide: points
 //               of one bin in one cycle lie in such a window, and the rounded
 //               cycle index takes at most floor(T / P) + 2 values.  High words
-//               sum to < M * 2^(26 - lobits) <= 2^(3b - 6) <= 2^30.
+//               sum to < M * 2^(27 - lobits) <= 2^(3b - 5) <= 2^31.
 //   Checked tight: uniform weights with no proven bound, but few points per bin
 //               on average (below kCheckedTightAvg per real bin at the grid's
 //               coarsest binning): the tight words with b = 12, and every
@@ -104,7 +104,8 @@ constexpr double kCheckedTightAvg = 1024.0;
 // overflow for the curve's point count n (bitlen = bits of n):
 //   low sums  < n * 2^lobits            <= 2^32
 //   high sums < n * 2^(qbits - lobits)  <= 2^31
-// with lobits = 32 - bitlen and qbits = min(26, 63 - 2*bitlen).
+// with lobits = 32 - bitlen and qbits = min(27, 63 - 2*bitlen) (27 is the most
+// the two-word layouts hold with up to 2^12 - 1 points per bin).
 struct CurveStat {
     double t_start;
     double shift;
@@ -216,7 +217,7 @@ __device__ __forceinline__ int q_scale(double m, int qbits) {
 
 __device__ __forceinline__ int bitlen64(long long n) { return n <= 0 ? 0 : 64 - __clzll(n); }
 __device__ __forceinline__ int curve_lobits(long long n) { return min(30, 32 - bitlen64(n)); }
-__device__ __forceinline__ int curve_qbits(long long n) { return min(26, 63 - 2 * bitlen64(n)); }
+__device__ __forceinline__ int curve_qbits(long long n) { return min(27, 63 - 2 * bitlen64(n)); }
 
 // Staged order of a curve's points.  Interleaved (n_full > 0): in every
 // whole chunk of kChunk points the kR staged values of lane l are points l,
@@ -494,10 +495,10 @@ __global__ void __launch_bounds__(kStageBlock) stage_kernel(const StageArgs a) {
     int packmode = uniform ? kPackCount : kPackSplit;
     int tight_bits = 64;
     if (uniform && a.periods) tight_bits = occupancy_bits(a, c, t, n, shd, shl);
-    if (uniform && tight_bits <= kTightMaxBits && qbits <= 26) packmode = kPackTight;
+    if (uniform && tight_bits <= kTightMaxBits && qbits <= 27) packmode = kPackTight;
     // no proven bound: the checked tight layout where bins are sparse on average
     bool tcheck = false;
-    if (uniform && packmode != kPackTight && a.periods && qbits <= 26 && n < (1LL << 24) &&
+    if (uniform && packmode != kPackTight && a.periods && qbits <= 27 && n < (1LL << 24) &&
         checked_tight_ok(a, c, n, shd)) {
         packmode = kPackTight;
         tight_bits = kTightMaxBits;

@@ -74,6 +74,23 @@ typedef struct { double c, f; } bin2;
  * vbls_v42_parity.cu:78-84   padding copy and serial prefix
  * vbls_v42_parity.cu:97-129  windows, dip-only, SNR
  */
+/* Pairwise sum of w[i] (what = 0) or y[i] * w[i] (what = 1) over [0, n),
+ * w NULL = unit weights: an error of O(log n) ulp. */
+static double pairwise_sum(int64_t n, const double* y, const double* w, int what)
+{
+    if (n <= 16) {
+        double s = 0.0;
+        for (int64_t i = 0; i < n; ++i) {
+            const double wi = w ? w[i] : 1.0;
+            s += what ? y[i] * wi : wi;
+        }
+        return s;
+    }
+    const int64_t h = n / 2;
+    return pairwise_sum(h, y, w, what) +
+           pairwise_sum(n - h, y + h, w ? w + h : NULL, what);
+}
+
 static void ref_binned_period(int64_t n, const double* dt, const double* y, const double* w,
                               double tot_w, double tot_y, double t_start, double period,
                               double bin_dur, double inv_bin_dur, int oversample, int max_bins,
@@ -160,13 +177,14 @@ int orc_ref_binned(int64_t n, const double* t, const double* y, const double* w,
     const double t_start = t[0];
     double* dt = (double*)malloc(sizeof(double) * (size_t)n);
     if (!dt) return ORC_ENOMEM;
-    double tot_w = 0.0, tot_y = 0.0; /* v42_parity.py:66-67 */
-    for (int64_t i = 0; i < n; ++i) {
-        dt[i] = t[i] - t_start;
-        const double wi = w ? w[i] : 1.0;
-        tot_w += wi;
-        tot_y += y[i] * wi;
-    }
+    for (int64_t i = 0; i < n; ++i) dt[i] = t[i] - t_start;
+    /* v42_parity.py:66-67: cp.sum(weights) and cp.sum(flux * weights), parallel
+     * tree reductions; pairwise sums stand in for them (a sequential sum of n
+     * equal weights drifts by up to n/2 ulp, which the kernel's
+     * y_out = (tot_y - y_in_sum) / (tot_w - ivar_in) turns into a relative
+     * depth error of order n * ulp / depth for sums near n * w) */
+    const double tot_w = pairwise_sum(n, y, w, 0);
+    const double tot_y = pairwise_sum(n, y, w, 1);
     /* vbls_v42_parity.cu:36-41 */
     double min_dur = durations[0];
     for (int k = 1; k < nd; ++k)
@@ -297,13 +315,11 @@ int orc_ref_fixed(int64_t n, const double* t, const double* y, const double* w, 
     double* f = (double*)malloc(sizeof(double) * (size_t)n);
     double* ww = (double*)malloc(sizeof(double) * (size_t)n);
     if (!t_rel || !f || !ww) { free(t_rel); free(f); free(ww); return ORC_ENOMEM; }
-    /* gpu_bls.py:60-69 -- weights, weighted-mean subtraction */
-    double w_sum = 0.0, wy_sum = 0.0;
-    for (int64_t i = 0; i < n; ++i) {
-        ww[i] = w ? w[i] : 1.0;
-        w_sum += ww[i];
-        wy_sum += y[i] * ww[i];
-    }
+    /* gpu_bls.py:60-69 -- weights, weighted-mean subtraction (cp.sum: tree
+     * reductions, restated as pairwise sums) */
+    for (int64_t i = 0; i < n; ++i) ww[i] = w ? w[i] : 1.0;
+    const double w_sum = pairwise_sum(n, y, ww, 0);
+    const double wy_sum = pairwise_sum(n, y, ww, 1);
     const double w_mean = wy_sum / w_sum;
     const double t_start = t[0]; /* gpu_bls.py:121 */
     for (int64_t i = 0; i < n; ++i) {
@@ -340,13 +356,13 @@ int orc_ref_fixed(int64_t n, const double* t, const double* y, const double* w, 
 /* ------------------------------------------------------------------------- */
 
 /* Per-point fixed-point magnitude bound |q| <= 2^qbits with
- * qbits = min(26, 63 - 2*bitlen(n)), bitlen(n) = number of bits of the point
+ * qbits = min(27, 63 - 2*bitlen(n)), bitlen(n) = number of bits of the point
  * count n: the engine's 32-bit split histogram words cannot overflow. */
 static int eng_qbits(int64_t n)
 {
     const int bl = n > 0 ? 64 - __builtin_clzll((unsigned long long)n) : 0;
     const int b = 63 - 2 * bl;
-    return b < 26 ? b : 26;
+    return b < 27 ? b : 27;
 }
 
 typedef struct {

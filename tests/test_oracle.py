@@ -207,7 +207,7 @@ def test_engine_stage_is_order_independent():
     s1.pop("t_start"); s2.pop("t_start")
     assert s1 == s2
     assert np.array_equal(np.sort(qy), np.sort(qy2))
-    assert np.abs(qw).max() <= 2 ** 26 and np.abs(qy).max() <= 2 ** 26
+    assert np.abs(qw).max() <= 2 ** 27 and np.abs(qy).max() <= 2 ** 27
 
 
 def test_cap_reproduces_reference_pileup():
