@@ -689,6 +689,7 @@ struct GroupSmem {
     int fmode[kMaxG];    // fold mode of each period (kFold*)
     int redo[kMaxG];     // checked tight layout: the period's counts overflowed
     int n_redo;          // how many periods of the group are folded again
+    int any_chunk;       // some period of the group uses kFoldChunk
     long long slot[kMaxG];
     int dbins[kMaxDur];
     double dur[kMaxDur];
@@ -861,8 +862,9 @@ __device__ __forceinline__ void fold_ends(const double (&d)[kR], bool sorted, do
 // always fold point by point).
 // WIN: bin-range pass -- only slots lo .. lo+W-1 are kept, at entries
 // 0 .. W-1 of H (one period at offset 0).
-// G: the number of the group's periods to fold (its first G).
-template <int GEOM, bool GLOB, int MODE, bool WIN = false>
+// G: the number of the group's periods to fold (its first G).  CHUNK: some
+// period of the group uses kFoldChunk (groups without one run the plain loop).
+template <int GEOM, bool GLOB, int MODE, bool WIN = false, bool CHUNK = false>
 __device__ void fold_group(const SearchArgs& a, const GroupSmem& gs, uint4* H, long long so,
                            long long n_pad, const CurveStat& st, int G, int lo = 0,
                            unsigned W = 0) {
@@ -925,7 +927,7 @@ __device__ void fold_group(const SearchArgs& a, const GroupSmem& gs, uint4* H, l
             const int2 nbb = gs.NBB[g];
             uint4* H0 = H + nbb.y;
             const unsigned base0 = GLOB ? 0u : (unsigned)__cvta_generic_to_shared(H0);
-            if (!GLOB && !WIN) {
+            if (CHUNK && !GLOB && !WIN) {
                 const int fm = gs.fmode[g];  // the same for every lane
                 if (fm != kFoldPoint) {
                     unsigned e0;
@@ -1695,6 +1697,20 @@ __device__ void finalize_group(const SearchArgs& a, GroupSmem& gs, longlong2* H,
     __syncthreads();
 }
 
+// The group's fold in the curve's own layout (shared-memory histograms when
+// CHUNK, GLOB otherwise: CHUNK is only used with shared memory).
+template <int GEOM, bool CHUNK, bool GLOB = false>
+__device__ __forceinline__ void fold_layout(const SearchArgs& a, const GroupSmem& gs, uint4* HU,
+                                            long long so, long long n_pad, const CurveStat& st,
+                                            int G) {
+    if (st.packmode == kPackTight)
+        fold_group<GEOM, GLOB, kPackTight, false, CHUNK>(a, gs, HU, so, n_pad, st, G);
+    else if (st.packmode == kPackCount)
+        fold_group<GEOM, GLOB, kPackCount, false, CHUNK>(a, gs, HU, so, n_pad, st, G);
+    else
+        fold_group<GEOM, GLOB, kPackSplit, false, CHUNK>(a, gs, HU, so, n_pad, st, G);
+}
+
 template <int GEOM, bool GLOB>
 __device__ void run_group(const SearchArgs& a, GroupSmem& gs, longlong2* H, const CurveStat& st,
                           long long so, long long n_pad, int nd) {
@@ -1705,14 +1721,17 @@ __device__ void run_group(const SearchArgs& a, GroupSmem& gs, longlong2* H, cons
     // global histograms fold a checked tight curve in the count layout at once
     const bool cview = GLOB && st.tcheck;
     const int G = gs.G;
-    if (cview)
-        fold_group<GEOM, GLOB, kPackCountT>(a, gs, HU, so, n_pad, st, G);
-    else if (st.packmode == kPackTight)
-        fold_group<GEOM, GLOB, kPackTight>(a, gs, HU, so, n_pad, st, G);
-    else if (st.packmode == kPackCount)
-        fold_group<GEOM, GLOB, kPackCount>(a, gs, HU, so, n_pad, st, G);
-    else
-        fold_group<GEOM, GLOB, kPackSplit>(a, gs, HU, so, n_pad, st, G);
+    if constexpr (GLOB) {
+        if (cview)
+            fold_group<GEOM, GLOB, kPackCountT>(a, gs, HU, so, n_pad, st, G);
+        else
+            fold_layout<GEOM, false, GLOB>(a, gs, HU, so, n_pad, st, G);
+    } else {
+        if (gs.any_chunk)
+            fold_layout<GEOM, true>(a, gs, HU, so, n_pad, st, G);
+        else
+            fold_layout<GEOM, false>(a, gs, HU, so, n_pad, st, G);
+    }
     __syncthreads();
     finalize_group<GEOM>(a, gs, H, st, nd, G, cview);
     if (!GLOB && st.tcheck) {
@@ -1741,7 +1760,10 @@ __device__ void run_group(const SearchArgs& a, GroupSmem& gs, longlong2* H, cons
                 for (int i = threadIdx.x; i < cnt; i += kBlock) H[off + i] = make_longlong2(0, 0);
             }
             __syncthreads();
-            fold_group<GEOM, false, kPackCountT>(a, gs, HU, so, n_pad, st, r);
+            if (gs.any_chunk)
+                fold_group<GEOM, false, kPackCountT, false, true>(a, gs, HU, so, n_pad, st, r);
+            else
+                fold_group<GEOM, false, kPackCountT>(a, gs, HU, so, n_pad, st, r);
             __syncthreads();
             finalize_group<GEOM>(a, gs, H, st, nd, r, true);
         }
@@ -1835,14 +1857,17 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) search_kernel(const Search
                 // fold mode per period: expected time-ordered points per bin
                 // (the plain staged order holds consecutive points per lane)
                 const bool dense_ok = gs.safe_floor && !gs.glob && !st.ilv;
+                int any_chunk = 0;
                 for (int k = 0; k < g; ++k) {
                     const double bw = (GEOM == ATB_GEOM_BINNED)
                                           ? st.bin_dur
                                           : gs.PIP[k].x / (double)gs.NBB[k].x;
                     const double run = bw * st.density;
                     gs.fmode[k] = dense_ok && run >= a.merge_run ? kFoldChunk : kFoldPoint;
+                    any_chunk |= gs.fmode[k];
                     gs.redo[k] = 0;
                 }
+                gs.any_chunk = any_chunk;
             }
             __syncthreads();
             if (gs.glob == 2) {
