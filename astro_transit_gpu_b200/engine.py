@@ -559,6 +559,9 @@ class BatchSession:
         self.plan = engine.plan(self.batch, config, self.outputs)
         self.step_graph = None    # H2D copies + search + D2H copies
         self.search_graph = None  # the search alone (inputs resident)
+        # recorded after each step: load() waits for it before it overwrites
+        # the pinned inputs the step's copies read
+        self._step_done: Optional[torch.cuda.Event] = None
 
     @property
     def h2d_bytes(self) -> int:
@@ -569,7 +572,11 @@ class BatchSession:
         return sum(v.numel() * v.element_size() for v in self.host_out.values())
 
     def load(self, t: np.ndarray, y: np.ndarray, w: Optional[np.ndarray] = None) -> None:
-        """Fill the pinned host input buffers (flattened, curve after curve)."""
+        """Fill the pinned host input buffers (flattened, curve after curve).
+        Waits first for the last step enqueued by :meth:`run`, whose
+        host-to-device copies read these buffers."""
+        if self._step_done is not None:
+            self._step_done.synchronize()
         self.host["t"].numpy()[:] = np.ravel(t)
         self.host["y"].numpy()[:] = np.ravel(y)
         if "w" in self.host:
@@ -609,6 +616,9 @@ class BatchSession:
                 self.step_graph.replay()
             else:
                 self._enqueue_step(s)
+        if self._step_done is None:
+            self._step_done = torch.cuda.Event()
+        self._step_done.record(s)
         return self.host_out
 
     def search(self, stream: Optional[torch.cuda.Stream] = None) -> None:

@@ -446,6 +446,14 @@ def test_batch_session_graph_replay_matches_eager(engine):
     torch.cuda.synchronize()
     for k in ref:
         assert torch.equal(graphed.host_out[k], eager.host_out[k]), k
+    # load() straight after run(), with no synchronisation, waits for the
+    # step's copies: the step still searches the inputs it was started with
+    graphed.load(t, y, w)
+    graphed.run()
+    graphed.load(t[::-1], y[::-1], w[::-1])
+    torch.cuda.synchronize()
+    for k in ref:
+        assert torch.equal(graphed.host_out[k], ref[k]), k
 
 
 @pytest.mark.parametrize("graphs", [False, True])
