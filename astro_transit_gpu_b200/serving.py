@@ -137,6 +137,10 @@ class BLSServer:
         self._max_held = 0
         self._expired = 0
         self._cancelled = 0
+        # the queue is pruned only when a client cancelled a request or the
+        # earliest admission deadline has passed (not on every poll)
+        self._cancel_seen = False
+        self._next_deadline = float("inf")
         self._worker = threading.Thread(target=self._run, name="bls-server", daemon=True)
         self._worker.start()
 
@@ -176,12 +180,20 @@ class BLSServer:
                        deadline=None if timeout is None else now + float(timeout))
         if req.nbytes > self.memory_budget:
             raise MemoryError(f"request needs {req.nbytes} bytes, budget {self.memory_budget}")
+        req.future.add_done_callback(self._on_done)
         with self._cv:
             if self._stop:
                 raise RuntimeError("server is closed")
             self._pending.append(req)
+            if req.deadline is not None:
+                self._next_deadline = min(self._next_deadline, req.deadline)
             self._cv.notify()
         return req.future
+
+    def _on_done(self, fut: Future) -> None:
+        if fut.cancelled():
+            with self._cv:
+                self._cancel_seen = True
 
     def stats(self) -> Dict[str, float]:
         with self._cv:
@@ -298,10 +310,16 @@ class BLSServer:
             for b in [b for b in self._inflight if b.event.query()]:
                 self._inflight.remove(b)
                 self._finish(b)
+            expired = []
             with self._cv:
-                self._pending, expired, cancelled = prune(self._pending, time.perf_counter())
-                self._expired += len(expired)
-                self._cancelled += len(cancelled)
+                now = time.perf_counter()
+                if self._cancel_seen or now > self._next_deadline:
+                    self._cancel_seen = False
+                    self._pending, expired, cancelled = prune(self._pending, now)
+                    self._expired += len(expired)
+                    self._cancelled += len(cancelled)
+                    self._next_deadline = min((r.deadline for r in self._pending
+                                               if r.deadline is not None), default=float("inf"))
             for r in expired:
                 try:
                     r.future.set_exception(TimeoutError(
