@@ -508,7 +508,12 @@ class BLSEngine:
 
 def split_outputs(batch: CurveBatch, outputs: Dict[str, torch.Tensor]) -> List[Dict[str, np.ndarray]]:
     """Host copies of the outputs, one dict per curve."""
-    host = {k: v.cpu().numpy() for k, v in outputs.items()}
+    return split_host_outputs(batch, {k: v.cpu().numpy() for k, v in outputs.items()})
+
+
+def split_host_outputs(batch: CurveBatch, host: Dict[str, np.ndarray]) -> List[Dict[str, np.ndarray]]:
+    """One dict per curve of views into host output arrays (every output field
+    and, when present, the per-curve best index)."""
     res = []
     for c in range(batch.n_curves):
         b, n = int(batch.out_begin[c]), int(batch.period_count[c])

@@ -36,7 +36,7 @@ from typing import Dict, List, Optional
 import numpy as np
 import torch
 
-from .engine import BLSEngine, CurveBatch, SearchConfig, split_outputs
+from .engine import BLSEngine, CurveBatch, SearchConfig, split_host_outputs
 
 
 @dataclass(eq=False)
@@ -63,6 +63,7 @@ class _Batch:
     stream: torch.cuda.Stream
     event: torch.cuda.Event
     nbytes: int
+    host_out: Dict[str, torch.Tensor]  # pinned copies of the outputs, valid after `event`
 
 
 def admit(pending, key, held: int, budget: int, max_batch: int):
@@ -261,14 +262,20 @@ class BLSServer:
                 weights=[r.w for r in reqs] if reqs[0].w is not None else None)
             plan = self.engine.plan(batch, reqs[0].config, stream=stream)
             plan.execute(stream)
+            # outputs back to pinned host memory in the batch's stream order, so
+            # the worker only slices them once the batch's event has fired
+            host_out = {k: torch.empty(v.shape, dtype=v.dtype, pin_memory=True)
+                        for k, v in plan.outputs.items()}
+            for k, v in plan.outputs.items():
+                host_out[k].copy_(v, non_blocking=True)
             ev = torch.cuda.Event()
             ev.record(stream)
-        return _Batch(reqs, batch, plan, stream, ev, sum(r.nbytes for r in reqs))
+        return _Batch(reqs, batch, plan, stream, ev, sum(r.nbytes for r in reqs), host_out)
 
     def _finish(self, b: _Batch) -> None:
         try:
             b.plan.check()
-            outs = split_outputs(b.batch, b.plan.outputs)
+            outs = split_host_outputs(b.batch, {k: v.numpy() for k, v in b.host_out.items()})
             err = None
         except Exception as e:  # invalid data: every request of the batch fails
             outs, err = None, e
