@@ -275,7 +275,12 @@ class BLSServer:
     def _finish(self, b: _Batch) -> None:
         try:
             b.plan.check()
-            outs = split_host_outputs(b.batch, {k: v.numpy() for k, v in b.host_out.items()})
+            # each request gets its own copy: the batch's pinned buffers go back
+            # to the host allocator's cache now, however long clients keep results
+            outs = [{k: v.copy() if isinstance(v, np.ndarray) else v for k, v in d.items()}
+                    for d in split_host_outputs(b.batch,
+                                                {k: v.numpy() for k, v in b.host_out.items()})]
+            b.host_out = {}
             err = None
         except Exception as e:  # invalid data: every request of the batch fails
             outs, err = None, e

@@ -378,20 +378,36 @@ def run_serving(device, rate, seconds, pool, seed=4001):
         # scanned by the collector while the requests run, as in a server
         gc.collect()
         gc.freeze()
+        # completions are counted, not kept: a client drops each result as a
+        # server's client would (holding every result of a long run at 2000
+        # requests/s would hold ~100 GB of host memory)
+        lock, all_done = threading.Lock(), threading.Event()
+        state = {"done": 0, "error": None}
+
+        def on_done(fut):
+            err = fut.exception()
+            with lock:
+                state["done"] += 1
+                if err is not None and state["error"] is None:
+                    state["error"] = err
+                if state["done"] == n_req:
+                    all_done.set()
+
         try:
             t0 = time.perf_counter()
             due = t0 + np.cumsum(gaps)
-            futs = []
             for i, d in zip(picks, due):
                 wait = d - time.perf_counter()
                 if wait > 0:
                     time.sleep(wait)
-                futs.append(srv.submit(**pool[int(i)]))
-            for f in futs:
-                f.result(timeout=3600)
+                srv.submit(**pool[int(i)]).add_done_callback(on_done)
+            if not all_done.wait(timeout=3600):
+                raise TimeoutError("serving requests did not complete")
             wall = time.perf_counter() - t0
         finally:
             gc.unfreeze()
+        if state["error"] is not None:
+            raise state["error"]
         st = srv.stats()
     return {"arrivals": "Poisson", "offered_rate_per_s": rate, "requests": n_req,
             "seconds": seconds, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
