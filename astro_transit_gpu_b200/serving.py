@@ -120,7 +120,7 @@ class BLSServer:
     """
 
     def __init__(self, device=0, memory_budget: float = 120e9, max_batch: int = 512,
-                 n_streams: int = 2):
+                 n_streams: int = 4):
         self.engine = BLSEngine.get(device)
         self.device = self.engine.device
         self.memory_budget = int(memory_budget)

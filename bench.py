@@ -97,6 +97,8 @@ def parse(argv=None):
                     help="comma-separated arrival rates of a serving sweep (e.g. "
                          "50,200,1000,2000), each for --serving-seconds, compared with a "
                          "one-call-per-curve loop over the same requests")
+    ap.add_argument("--serving-streams", type=int, default=4,
+                    help="batches the server keeps in flight (one CUDA stream each)")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--launch-check", action="store_true",
                     help="start the ranks, report the world size every rank sees, exit "
@@ -356,7 +358,7 @@ def serving_pool(n, seed=4000):
     return pool
 
 
-def run_serving(device, rate, seconds, pool, seed=4001):
+def run_serving(device, rate, seconds, pool, seed=4001, n_streams=4):
     """Continuous-batching server under Poisson arrivals at `rate` requests/s
     for `seconds`: each request is a curve drawn from `pool`; returns p50/p99
     latency from submission to result and the completed rate."""
@@ -367,7 +369,8 @@ def run_serving(device, rate, seconds, pool, seed=4001):
     picks = (rng.permutation(len(pool))[:n_req] if n_req <= len(pool)
              else rng.integers(0, len(pool), n_req))
     gaps = rng.exponential(1.0 / rate, n_req)
-    with BLSServer(device=device, memory_budget=120e9, max_batch=512, n_streams=2) as srv:
+    with BLSServer(device=device, memory_budget=120e9, max_batch=512,
+                   n_streams=n_streams) as srv:
         # warm-up (library load, allocator pools at the sizes of large
         # batches): one request, then a burst of 64 at once; not timed
         srv.submit(**pool[0]).result(timeout=300)
@@ -417,7 +420,7 @@ def run_serving(device, rate, seconds, pool, seed=4001):
                        "(N log-U[1e3, 2e5], 1-13 sectors, 1000-60000 periods), fast method, "
                        "4-8 durations 0.02-0.30 d",
             "admission": "120 GB device-memory budget, up to 512 requests per batch, "
-                         "2 batches in flight"}
+                         f"{n_streams} batches in flight"}
 
 
 def per_call_rate(device, pool, n=500):
@@ -657,10 +660,12 @@ def main(argv=None):
                  else [])
         pool = serving_pool(min(SERVING_POOL, max(64, int(max([args.serving_rate] + rates)
                                                               * args.serving_seconds))))
-        line["serving"] = run_serving(dev, args.serving_rate, args.serving_seconds, pool)
+        line["serving"] = run_serving(dev, args.serving_rate, args.serving_seconds, pool,
+                                      n_streams=args.serving_streams)
         if rates:
             line["serving_sweep"] = {
-                "rates": [run_serving(dev, r, args.serving_seconds, pool) for r in rates],
+                "rates": [run_serving(dev, r, args.serving_seconds, pool,
+                                      n_streams=args.serving_streams) for r in rates],
                 "per_call_path": per_call_rate(dev, pool)}
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload != "precision":
         rate, cores, sample, outs, _ = cpu_reference(wl, args.method, args.cpu_seconds)
