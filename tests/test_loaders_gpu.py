@@ -1,10 +1,12 @@
 """GPU tests: a sector-cache batch (shared time axis, padding dropped) and the
 batched injection/recovery grid give the same results as one search per
-curve."""
+curve, and those results are the oracle's (its mirror of the engine
+arithmetic), bit for bit."""
 import numpy as np
 import pytest
 
 import recipes as R
+from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
@@ -38,8 +40,14 @@ def test_sector_cache_batch_equals_per_target_searches(engine, tmp_path):
             ref_b = CurveBatch.from_arrays([sc.times[i]], [sc.fluxes[i]], [sc.flux_errs[i]],
                                            periods=periods, durations=durs, device=engine.device)
             ref = split_outputs(ref_b, engine.search(ref_b, cfg))[0]
+            w = (1.0 / (np.asarray(sc.flux_errs[i], np.float64) ** 2)).astype(np.float32)
+            y = np.asarray(sc.fluxes[i], np.float32)
+            ora = (O.eng_fixed(sc.times[i], y, w, periods, durs, n_bins=200)
+                   if cfg.method == "fast" else
+                   O.eng_binned(sc.times[i], y, w, periods, durs, objective="snr"))
             for k in FIELDS:
                 assert np.array_equal(got[i][k], ref[k]), (cfg.method, i, k)
+                assert np.array_equal(got[i][k], ora[k]), (cfg.method, i, k, "oracle")
     # the injected transit is found
     b = sc.batch(periods, durs, device=engine.device)
     o = split_outputs(b, engine.search(b, SearchConfig("fast", n_bins=200)))[1]
@@ -65,7 +73,12 @@ def test_injection_recovery_batch_equals_one_search_per_trial(engine):
         for d in (3e-3, 1e-2):
             for trial in range(3):
                 t0 = t[0] + rng.random() * p
-                res = run_gpu_bls(t, inject_box_transit(t, y, p, t0, 0.1, d), periods, durs)
+                yi = inject_box_transit(t, y, p, t0, 0.1, d)
+                res = run_gpu_bls(t, yi, periods, durs)
+                if trial == 0:
+                    ora = O.eng_fixed(t, np.asarray(yi), None, periods, durs, n_bins=200)
+                    assert np.array_equal(res["power"], ora["power"]), (p, d)
+                    assert np.array_equal(res["all_t0s"], ora["t0"]), (p, d)
                 row = df[(df.injected_period == p) & (df.injected_depth == d)
                          & (df.trial == trial)].iloc[0]
                 assert row.detected_period == res["best_period"]
