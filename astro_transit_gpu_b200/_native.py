@@ -49,7 +49,7 @@ _i32p = ctypes.POINTER(ctypes.c_int32)
 class Params(ctypes.Structure):
     _fields_ = [("geometry", _i32), ("objective", _i32), ("n_bins", _i32),
                 ("oversample", _i32), ("max_bins", _i32), ("tile_periods", _i32),
-                ("merge_run", _i32), ("reserved", _i32)]
+                ("merge_run", _i32), ("cta_threads", _i32)]
 
 
 class Batch(ctypes.Structure):

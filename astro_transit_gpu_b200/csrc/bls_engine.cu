@@ -51,13 +51,23 @@ namespace {
 #ifndef ATB_POINTS_PER_THREAD
 #define ATB_POINTS_PER_THREAD 4
 #endif
+// Search-CTA shapes: kBlock threads with kMinBlocks CTAs per SM (the default
+// for the astropy-binned geometry), or kBlockB threads with kMinBlocksB CTAs
+// per SM (the fixed-bin default; atb_params.cta_threads selects either).  The
+// device code takes the CTA size from blockDim.x; shared arrays are sized for
+// the larger shape.
 constexpr int kBlock = ATB_BLOCK;            // threads of a search CTA
 constexpr int kMinBlocks = ATB_MIN_BLOCKS;   // resident search CTAs per SM
-constexpr int kWarps = kBlock / 32;
+constexpr int kBlockB = 256;
+constexpr int kMinBlocksB = 4;
+constexpr int kMaxWarps = (kBlock > kBlockB ? kBlock : kBlockB) / 32;
 // Teams of tw warps (tw a power of two) must tile the CTA exactly, so that
 // every warp of a team reaches the team's named barrier.
-static_assert(kBlock % 32 == 0 && kWarps >= 2 && kWarps <= 32 && (kWarps & (kWarps - 1)) == 0,
+static_assert(kBlock % 32 == 0 && kBlock / 32 >= 2 && kBlock / 32 <= 32 &&
+                  ((kBlock / 32) & (kBlock / 32 - 1)) == 0 && kBlockB / 32 >= 2 &&
+                  ((kBlockB / 32) & (kBlockB / 32 - 1)) == 0,
               "search CTA: a power-of-two number of warps, at most 1024 threads");
+constexpr int kBenchBlock = 512;  // threads of the microbenchmark kernels
 constexpr int kR = ATB_POINTS_PER_THREAD;    // consecutive points a thread holds in registers
 constexpr int kTileP = 64;             // periods per work-queue tile
 constexpr int kMaxG = 64;              // periods per shared-memory group
@@ -65,6 +75,10 @@ constexpr int kMaxDur = 32;            // durations per curve
 constexpr int kStageAlign = 32;        // staged curves start at multiples of 32 points
 constexpr int kStageBlock = 256;
 constexpr double kDefaultMergeRun = 8.0;   // atb_params.merge_run = 0
+// atb_params.cta_threads = 0 with fixed bins: four 256-thread CTAs per SM
+// (measured faster than two 512-thread ones for fixed bins; slower for the
+// binned geometry, whose larger histograms want the bigger shared-memory share)
+constexpr int kDefaultFixedThreads = kBlockB;
 constexpr int kChunk = 32 * kR;        // staged points of one warp's fold step
 constexpr double kMagicSlot = 4503599627370497.0;   // 2^52 + 1: x + C (rz) = 2^52 + int(x) + 1, x in (-1, 2^31 - 1)
 constexpr double kMagicFloor = 6755399441055744.0;  // 1.5*2^52: (m + C)(rd) - C = floor(m), |m| < 2^50
@@ -693,11 +707,11 @@ struct GroupSmem {
     long long slot[kMaxG];
     int dbins[kMaxDur];
     double dur[kMaxDur];
-    int L[kWarps][kMaxDur];
-    longlong2 scan[kWarps];
-    float num[kWarps];
-    float den[kWarps];
-    int key[kWarps];
+    int L[kMaxWarps][kMaxDur];
+    longlong2 scan[kMaxWarps];
+    float num[kMaxWarps];
+    float den[kMaxWarps];
+    int key[kMaxWarps];
     long long tile;
     long long pb, pe, pn;
     int curve;
@@ -872,7 +886,8 @@ __device__ void fold_group(const SearchArgs& a, const GroupSmem& gs, uint4* H, l
     // split position of the layout's words (count layout for kPackCountT)
     const int L = MODE == kPackCountT ? curve_lobits(st.n_cnt) : st.lobits;
     const unsigned lomask = (1u << L) - 1u;
-    for (long long base = 0; base < n_pad; base += (long long)kBlock * kR) {
+    const int nt = (int)blockDim.x;
+    for (long long base = 0; base < n_pad; base += (long long)nt * kR) {
         const long long i0 = base + (long long)threadIdx.x * kR;
         if (i0 >= n_pad) continue;
         double d[kR];
@@ -1557,8 +1572,8 @@ __device__ void run_period_binned_passes(const SearchArgs& a, GroupSmem& gs, lon
     const int S = W - Lmax;  // >= 1: checked when the group was formed
     Team tm;
     tm.id = 0;
-    tm.nwarps = kWarps;
-    tm.nthreads = kBlock;
+    tm.nwarps = (int)(blockDim.x >> 5);
+    tm.nthreads = (int)blockDim.x;
     tm.warp0 = 0;
     tm.tid = threadIdx.x;
     const bool cnt = st.cnt_win != 0;
@@ -1582,7 +1597,7 @@ __device__ void run_period_binned_passes(const SearchArgs& a, GroupSmem& gs, lon
     }
     uint4* HU = reinterpret_cast<uint4*>(H);
     for (int lo = 0; lo < NB; lo += S) {
-        for (int i = threadIdx.x; i < W; i += kBlock) H[i] = make_longlong2(0, 0);
+        for (int i = threadIdx.x; i < W; i += blockDim.x) H[i] = make_longlong2(0, 0);
         __syncthreads();
         if (cview)
             fold_group<ATB_GEOM_BINNED, false, kPackCountT, true>(a, gs, HU, so, n_pad, st, 1, lo, W);
@@ -1683,9 +1698,10 @@ __device__ void finalize_group(const SearchArgs& a, GroupSmem& gs, longlong2* H,
     // measured slower); multi-warp teams synchronise on named barriers 1..15,
     // so at most 15 of them may exist
     int tw = 1;
-    while (tw * 2 * G <= kWarps) tw *= 2;
-    while (tw > 1 && kWarps / tw > 15) tw *= 2;
-    const int n_teams = kWarps / tw;
+    const int nw = (int)(blockDim.x >> 5);
+    while (tw * 2 * G <= nw) tw *= 2;
+    while (tw > 1 && nw / tw > 15) tw *= 2;
+    const int n_teams = nw / tw;
     const int warp = threadIdx.x >> 5;
     Team tm;
     tm.id = warp / tw;
@@ -1715,7 +1731,7 @@ template <int GEOM, bool GLOB>
 __device__ void run_group(const SearchArgs& a, GroupSmem& gs, longlong2* H, const CurveStat& st,
                           long long so, long long n_pad, int nd) {
     const int total = gs.total;
-    for (int i = threadIdx.x; i < total; i += kBlock) H[i] = make_longlong2(0, 0);
+    for (int i = threadIdx.x; i < total; i += blockDim.x) H[i] = make_longlong2(0, 0);
     __syncthreads();
     uint4* HU = reinterpret_cast<uint4*>(H);
     // global histograms fold a checked tight curve in the count layout at once
@@ -1757,7 +1773,7 @@ __device__ void run_group(const SearchArgs& a, GroupSmem& gs, longlong2* H, cons
         if (r > 0) {
             for (int k = 0; k < r; ++k) {
                 const int off = gs.NBB[k].y, cnt = gs.NBB[k].x + 2;
-                for (int i = threadIdx.x; i < cnt; i += kBlock) H[off + i] = make_longlong2(0, 0);
+                for (int i = threadIdx.x; i < cnt; i += blockDim.x) H[off + i] = make_longlong2(0, 0);
             }
             __syncthreads();
             if (gs.any_chunk)
@@ -1770,8 +1786,8 @@ __device__ void run_group(const SearchArgs& a, GroupSmem& gs, longlong2* H, cons
     }
 }
 
-template <int GEOM>
-__global__ void __launch_bounds__(kBlock, kMinBlocks) search_kernel(const SearchArgs a) {
+template <int GEOM, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) search_kernel(const SearchArgs a) {
     extern __shared__ __align__(16) longlong2 s_hist[];
     __shared__ GroupSmem gs;
 
@@ -1809,7 +1825,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) search_kernel(const Search
         long long pn = gs.pb;
         const long long pe = gs.pe;
         // the tile's periods and bin counts, loaded in parallel
-        for (int i = threadIdx.x; i < (int)(pe - pn); i += kBlock) {
+        for (int i = threadIdx.x; i < (int)(pe - pn); i += NT) {
             double P = a.periods[pbeg + pn + i];
             if (!(P > 0.0) || !(P < 1.0e300)) {
                 atomicOr(a.status, 4);
@@ -2073,7 +2089,7 @@ constexpr int kBenchSlots = 4096;  // counters of the reduction benchmark
 // each warp's lanes hit 32 consecutive counters (conflict-free), pattern 1 =
 // pseudo-random counters.
 template <bool WIDE>
-__global__ void __launch_bounds__(kBlock) bench_smem_red_kernel(int iters, int pattern,
+__global__ void __launch_bounds__(kBenchBlock) bench_smem_red_kernel(int iters, int pattern,
                                                                 unsigned long long* sink) {
     __shared__ unsigned long long h[kBenchSlots];
     for (int i = threadIdx.x; i < kBenchSlots; i += blockDim.x) h[i] = 0;
@@ -2098,7 +2114,7 @@ __global__ void __launch_bounds__(kBlock) bench_smem_red_kernel(int iters, int p
 }
 
 // FP64 fused multiply-add throughput: 8 independent chains per thread
-__global__ void __launch_bounds__(kBlock) bench_dfma_kernel(int iters, double* sink) {
+__global__ void __launch_bounds__(kBenchBlock) bench_dfma_kernel(int iters, double* sink) {
     double a[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) a[k] = 1.0 + 1e-9 * (threadIdx.x + k);
@@ -2139,6 +2155,8 @@ struct atb_plan {
     int y_is_f64 = 0;
     int grid = 0;
     int smem_bytes = 0;
+    int nt = kBlock;        // threads per search CTA
+    int minb = kMinBlocks;  // resident search CTAs per SM
     long long n_tiles = 0;
     std::vector<void*> allocs;
     long long scratch_bytes = 0;
@@ -2228,6 +2246,34 @@ double fold_threshold(int32_t v, double dflt) {
     return v == 0 ? dflt : (v < 0 ? 1.0e300 : (double)v);
 }
 
+// The search kernel's instance for a geometry and CTA size.
+using SearchFn = void (*)(const SearchArgs);
+SearchFn search_fn(int geom, int nt) {
+    if (geom == ATB_GEOM_BINNED)
+        return nt == kBlockB ? search_kernel<ATB_GEOM_BINNED, kBlockB, kMinBlocksB>
+                             : search_kernel<ATB_GEOM_BINNED, kBlock, kMinBlocks>;
+    return nt == kBlockB ? search_kernel<ATB_GEOM_FIXED, kBlockB, kMinBlocksB>
+                         : search_kernel<ATB_GEOM_FIXED, kBlock, kMinBlocks>;
+}
+
+// CTA shape from atb_params.cta_threads (0 = the geometry's default);
+// false for an unsupported size.
+bool plan_shape(const atb_params* prm, int* nt, int* minb) {
+    int v = prm->cta_threads;
+    if (v == 0) v = prm->geometry == ATB_GEOM_FIXED ? kDefaultFixedThreads : kBlock;
+    if (v == kBlock) {
+        *nt = kBlock;
+        *minb = kMinBlocks;
+        return true;
+    }
+    if (v == kBlockB) {
+        *nt = kBlockB;
+        *minb = kMinBlocksB;
+        return true;
+    }
+    return false;
+}
+
 int launch_stage(atb_plan* p, cudaStream_t s) {
     if (p->y_is_f64)
         stage_kernel<double><<<p->n_curves, kStageBlock, 0, s>>>(p->sa);
@@ -2247,9 +2293,9 @@ int bench_smem_red(atb_handle* h, int pattern, double* reductions_per_s) {
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
-    bench_smem_red_kernel<WIDE><<<grid, kBlock>>>(iters, pattern, sink);  // warm-up
+    bench_smem_red_kernel<WIDE><<<grid, kBenchBlock>>>(iters, pattern, sink);  // warm-up
     cudaEventRecord(a);
-    for (int r = 0; r < 5; ++r) bench_smem_red_kernel<WIDE><<<grid, kBlock>>>(iters, pattern, sink);
+    for (int r = 0; r < 5; ++r) bench_smem_red_kernel<WIDE><<<grid, kBenchBlock>>>(iters, pattern, sink);
     cudaEventRecord(b);
     cudaError_t e = cudaEventSynchronize(b);
     float ms = 0;
@@ -2258,7 +2304,7 @@ int bench_smem_red(atb_handle* h, int pattern, double* reductions_per_s) {
     cudaEventDestroy(b);
     cudaFree(sink);
     if (e != cudaSuccess) return fail(h, ATB_ECUDA, "bench: %s", cudaGetErrorString(e));
-    *reductions_per_s = 5.0 * grid * kBlock * (double)iters / (ms * 1e-3);
+    *reductions_per_s = 5.0 * grid * kBenchBlock * (double)iters / (ms * 1e-3);
     return ATB_OK;
 }
 
@@ -2353,6 +2399,10 @@ int plan_create(atb_handle* h, const atb_params* prm, const atb_batch* b, const 
     } else {
         return fail(h, ATB_EINVAL, "unknown geometry %d", prm->geometry);
     }
+    int cta_nt = kBlock, cta_minb = kMinBlocks;
+    if (!plan_shape(prm, &cta_nt, &cta_minb))
+        return fail(h, ATB_EINVAL, "cta_threads=%d: 0, %d or %d expected", prm->cta_threads,
+                    kBlock, kBlockB);
     if (!b->point_offset || !b->period_begin || !b->period_count || !b->dur_begin ||
         !b->dur_count || !b->out_begin)
         return fail(h, ATB_EINVAL, "batch index arrays must not be NULL");
@@ -2400,7 +2450,7 @@ int plan_create(atb_handle* h, const atb_params* prm, const atb_batch* b, const 
     // SMs idle)
     int tile_p = prm->tile_periods;
     if (tile_p < 1 || tile_p > kTileP) {
-        const long long slots = 4LL * h->n_sm * kMinBlocks;
+        const long long slots = 4LL * h->n_sm * cta_minb;
         tile_p = kTileP;
         while (tile_p > 8) {
             long long tiles = 0;
@@ -2422,6 +2472,8 @@ int plan_create(atb_handle* h, const atb_params* prm, const atb_batch* b, const 
     p->n_curves = nc;
     p->y_is_f64 = b->y_is_f64 ? 1 : 0;
     p->n_tiles = tile_off[nc];
+    p->nt = cta_nt;
+    p->minb = cta_minb;
 
     int rc = ATB_OK;
     long long *d_pt, *d_toff, *d_pbeg, *d_pcnt, *d_dbeg, *d_obeg, *d_soff, *d_tiles;
@@ -2469,8 +2521,8 @@ int plan_create(atb_handle* h, const atb_params* prm, const atb_batch* b, const 
 
     // shared-memory histogram capacity and the global fallback size
     const int static_smem = (int)sizeof(GroupSmem) + 64;
-    // kMinBlocks CTAs share the SM's shared memory (1 KiB per CTA is reserved)
-    int dyn = std::min(h->smem_optin, h->smem_per_sm / kMinBlocks - 1024) - static_smem;
+    // cta_minb CTAs share the SM's shared memory (1 KiB per CTA is reserved)
+    int dyn = std::min(h->smem_optin, h->smem_per_sm / cta_minb - 1024) - static_smem;
     dyn = dyn / 16 * 16;
     const int cap = dyn / 16;
     int nb_max = prm->n_bins;
@@ -2498,22 +2550,14 @@ int plan_create(atb_handle* h, const atb_params* prm, const atb_batch* b, const 
         }
     }
     int occ = 1;
-    cudaError_t e0 = cudaSuccess;
-    if (prm->geometry == ATB_GEOM_BINNED)
-        e0 = cudaFuncSetAttribute(search_kernel<ATB_GEOM_BINNED>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
-    else
-        e0 = cudaFuncSetAttribute(search_kernel<ATB_GEOM_FIXED>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+    const SearchFn sfn = search_fn(prm->geometry, cta_nt);
+    cudaError_t e0 = cudaFuncSetAttribute(sfn, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
     if (e0 != cudaSuccess) {
         plan_free(p);
         delete p;
         return fail(h, ATB_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e0));
     }
-    if (prm->geometry == ATB_GEOM_BINNED)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, search_kernel<ATB_GEOM_BINNED>, kBlock, dyn);
-    else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, search_kernel<ATB_GEOM_FIXED>, kBlock, dyn);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, sfn, cta_nt, dyn);
     occ = std::max(occ, 1);
     long long grid = (long long)h->n_sm * occ;
     grid = std::max(1LL, std::min(grid, p->n_tiles));
@@ -2592,10 +2636,7 @@ int atb_plan_execute(atb_plan* p, void* stream) {
     int rc = launch_stage(p, s);
     if (rc) return rc;
     if (p->n_tiles > 0) {
-        if (p->prm.geometry == ATB_GEOM_BINNED)
-            search_kernel<ATB_GEOM_BINNED><<<p->grid, kBlock, p->smem_bytes, s>>>(p->qa);
-        else
-            search_kernel<ATB_GEOM_FIXED><<<p->grid, kBlock, p->smem_bytes, s>>>(p->qa);
+        search_fn(p->prm.geometry, p->nt)<<<p->grid, p->nt, p->smem_bytes, s>>>(p->qa);
         ATB_CUDA(h, cudaGetLastError());
     }
     if (p->best) {
@@ -2817,10 +2858,7 @@ int atb_plan_profile(atb_plan* p, void* stream, float* ms_stage, float* ms_searc
     int rc = launch_stage(p, s);
     ATB_CUDA(h, cudaEventRecord(ev[1], s));
     if (!rc && p->n_tiles > 0) {
-        if (p->prm.geometry == ATB_GEOM_BINNED)
-            search_kernel<ATB_GEOM_BINNED><<<p->grid, kBlock, p->smem_bytes, s>>>(p->qa);
-        else
-            search_kernel<ATB_GEOM_FIXED><<<p->grid, kBlock, p->smem_bytes, s>>>(p->qa);
+        search_fn(p->prm.geometry, p->nt)<<<p->grid, p->nt, p->smem_bytes, s>>>(p->qa);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) rc = fail(h, ATB_ECUDA, "search launch: %s", cudaGetErrorString(e));
     }
@@ -2859,9 +2897,9 @@ int atb_bench_dfma(atb_handle* h, double* fma_per_s) {
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
-    bench_dfma_kernel<<<grid, kBlock>>>(iters, sink);
+    bench_dfma_kernel<<<grid, kBenchBlock>>>(iters, sink);
     cudaEventRecord(a);
-    for (int r = 0; r < 5; ++r) bench_dfma_kernel<<<grid, kBlock>>>(iters, sink);
+    for (int r = 0; r < 5; ++r) bench_dfma_kernel<<<grid, kBenchBlock>>>(iters, sink);
     cudaEventRecord(b);
     cudaError_t e = cudaEventSynchronize(b);
     float ms = 0;
@@ -2870,7 +2908,7 @@ int atb_bench_dfma(atb_handle* h, double* fma_per_s) {
     cudaEventDestroy(b);
     cudaFree(sink);
     if (e != cudaSuccess) return fail(h, ATB_ECUDA, "bench: %s", cudaGetErrorString(e));
-    *fma_per_s = 5.0 * grid * kBlock * 8.0 * (double)iters / (ms * 1e-3);
+    *fma_per_s = 5.0 * grid * kBenchBlock * 8.0 * (double)iters / (ms * 1e-3);
     return ATB_OK;
 }
 
@@ -2990,6 +3028,10 @@ extern "C" int atb_search_curve_static(const atb_params* prm, const double* t, c
     } else {
         return static_fail(err, err_len, ATB_EINVAL, "unknown geometry %d", prm->geometry);
     }
+    // one CTA shape here: its shared-memory size bounds the bin counts accepted
+    if (prm->cta_threads != 0 && prm->cta_threads != kBlock)
+        return static_fail(err, err_len, ATB_EINVAL, "cta_threads=%d: 0 or %d expected",
+                           prm->cta_threads, kBlock);
 
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     int dev = 0;
@@ -3021,10 +3063,10 @@ extern "C" int atb_search_curve_static(const atb_params* prm, const double* t, c
     if (e != cudaSuccess || !ptr)
         return static_fail(err, err_len, ATB_ECUDA, "cudaGetSymbolAddress: %s",
                            cudaGetErrorString(e));
-    e = cudaFuncSetAttribute(search_kernel<ATB_GEOM_BINNED>,
+    e = cudaFuncSetAttribute(search_kernel<ATB_GEOM_BINNED, kBlock, kMinBlocks>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(search_kernel<ATB_GEOM_FIXED>,
+        e = cudaFuncSetAttribute(search_kernel<ATB_GEOM_FIXED, kBlock, kMinBlocks>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
     if (e != cudaSuccess)
         return static_fail(err, err_len, ATB_ECUDA, "cudaFuncSetAttribute: %s",
@@ -3121,14 +3163,16 @@ extern "C" int atb_search_curve_static(const atb_params* prm, const double* t, c
     qa.status = &m->status;
     int occ = 1;
     if (prm->geometry == ATB_GEOM_BINNED)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, search_kernel<ATB_GEOM_BINNED>, kBlock, dyn);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &occ, search_kernel<ATB_GEOM_BINNED, kBlock, kMinBlocks>, kBlock, dyn);
     else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, search_kernel<ATB_GEOM_FIXED>, kBlock, dyn);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &occ, search_kernel<ATB_GEOM_FIXED, kBlock, kMinBlocks>, kBlock, dyn);
     const int grid = (int)std::max(1LL, std::min((long long)n_sm * std::max(occ, 1), n_tiles));
     if (prm->geometry == ATB_GEOM_BINNED)
-        search_kernel<ATB_GEOM_BINNED><<<grid, kBlock, dyn, s>>>(qa);
+        search_kernel<ATB_GEOM_BINNED, kBlock, kMinBlocks><<<grid, kBlock, dyn, s>>>(qa);
     else
-        search_kernel<ATB_GEOM_FIXED><<<grid, kBlock, dyn, s>>>(qa);
+        search_kernel<ATB_GEOM_FIXED, kBlock, kMinBlocks><<<grid, kBlock, dyn, s>>>(qa);
     if (best_index)
         best_kernel<<<1, 32, 0, s>>>(1, m->per_cnt, m->out_beg, power, nullptr, best_index);
     e = cudaGetLastError();

@@ -38,6 +38,9 @@ class SearchConfig:
                which a thread adds the points it holds once when they share a
                slot (0 = the default 8, or the value the autotuner found;
                < 0 = never).  Results never depend on it.
+    cta_threads  threads per search CTA: 512 (two CTAs per SM) or 256 (four
+               per SM); 0 = the geometry's default, or the autotuner's value.
+               Results never depend on it.
     """
     method: str = "parity"
     objective: Optional[str] = None
@@ -46,6 +49,7 @@ class SearchConfig:
     max_bins: Optional[int] = None
     tile_periods: int = 0
     merge_run: int = 0
+    cta_threads: int = 0
 
     def params(self) -> N.Params:
         if self.method == "fast":
@@ -53,7 +57,8 @@ class SearchConfig:
             if obj != "fast":
                 raise ValueError("method='fast' uses the reference's fast score")
             return N.Params(N.GEOM_FIXED, N.OBJ_FAST, int(self.n_bins), int(self.oversample), 0,
-                            int(self.tile_periods), int(self.merge_run), 0)
+                            int(self.tile_periods), int(self.merge_run),
+                            int(self.cta_threads))
         if self.method == "parity":
             obj = self.objective or "snr"
             if obj not in ("snr", "likelihood"):
@@ -61,7 +66,7 @@ class SearchConfig:
             mb = 0 if self.max_bins is None else int(self.max_bins)
             return N.Params(N.GEOM_BINNED, N.OBJECTIVES[obj], int(self.n_bins),
                             int(self.oversample), mb, int(self.tile_periods),
-                            int(self.merge_run), 0)
+                            int(self.merge_run), int(self.cta_threads))
         raise ValueError(f"unknown method {self.method!r} (expected 'fast' or 'parity')")
 
 
@@ -377,6 +382,8 @@ class BLSEngine:
 
     # fold strategies the autotuner tries (merge_run)
     FOLD_CANDIDATES = (0, -1, 4, 16)
+    # CTA sizes the autotuner tries (cta_threads)
+    SHAPE_CANDIDATES = (512, 256)
 
     def _time_search(self, batch: CurveBatch, cfg: SearchConfig, repeats: int) -> float:
         plan = SearchPlan(self, batch, cfg, self.allocate_outputs(batch))
@@ -389,31 +396,42 @@ class BLSEngine:
 
     def autotune(self, batch: CurveBatch, config: SearchConfig,
                  candidates: Sequence[int] = (8, 16, 32, 64),
-                 fold_candidates: Sequence[tuple] = FOLD_CANDIDATES, repeats: int = 2,
+                 fold_candidates: Sequence[int] = FOLD_CANDIDATES,
+                 shape_candidates: Sequence[int] = SHAPE_CANDIDATES, repeats: int = 2,
                  persist: bool = True) -> Dict[str, int]:
         """Time the search kernel on `batch` over the knobs that never change
-        a result -- first the tile sizes in `candidates` (periods per
-        work-queue tile), then, at the fastest of those, the fold strategies
-        in `fold_candidates` (merge_run values) -- keep the
+        a result -- first the CTA sizes in `shape_candidates` (cta_threads),
+        then, at the fastest of those, the tile sizes in `candidates`
+        (periods per work-queue tile), then the fold strategies in
+        `fold_candidates` (merge_run values) -- keep the
         fastest setting for this kind of batch (``tune_key``) in the engine's
         tuning table, written to its file unless `persist` is false, and
         return it.  Later plans whose config leaves a knob at 0 use the tuned
         value, in this process and in later ones."""
         times: Dict[str, float] = {}
+        best_nt, best_ms = int(config.cta_threads), None
+        for nt in shape_candidates:
+            ms = self._time_search(batch, replace(config, cta_threads=int(nt)), repeats)
+            times[f"cta={int(nt)}"] = ms
+            if best_ms is None or ms < best_ms:
+                best_nt, best_ms = int(nt), ms
         best_tp, best_ms = None, None
         for tp in candidates:
-            ms = self._time_search(batch, replace(config, tile_periods=int(tp)), repeats)
-            times[f"tile={int(tp)}"] = ms
+            cfg = replace(config, cta_threads=best_nt, tile_periods=int(tp))
+            ms = self._time_search(batch, cfg, repeats)
+            times[f"cta={best_nt},tile={int(tp)}"] = ms
             if best_ms is None or ms < best_ms:
                 best_tp, best_ms = int(tp), ms
         best_fold = int(config.merge_run)
         for mr in fold_candidates:
-            cfg = replace(config, tile_periods=best_tp, merge_run=int(mr))
+            cfg = replace(config, cta_threads=best_nt, tile_periods=best_tp, merge_run=int(mr))
             ms = self._time_search(batch, cfg, repeats)
-            times[f"tile={best_tp},merge_run={mr}"] = ms
+            times[f"cta={best_nt},tile={best_tp},merge_run={mr}"] = ms
             if ms < best_ms:
                 best_fold, best_ms = int(mr), ms
         settings = {"tile_periods": best_tp, "merge_run": best_fold}
+        if best_nt:
+            settings["cta_threads"] = best_nt
         self.tuning.put(self.tune_key(batch, config),
                         {**settings, "search_ms": times, "best_ms": best_ms})
         if persist:
@@ -427,7 +445,7 @@ class BLSEngine:
         tuned = self.tuning.get(self.tune_key(batch, config))
         if not tuned:
             return config
-        upd = {k: int(tuned[k]) for k in ("tile_periods", "merge_run")
+        upd = {k: int(tuned[k]) for k in ("tile_periods", "merge_run", "cta_threads")
                if k in tuned and getattr(config, k) == 0}
         return replace(config, **upd) if upd else config
 

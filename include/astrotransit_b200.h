@@ -66,7 +66,10 @@ typedef struct {
      * holds once when they provably share a slot.  0 = the default (8),
      * < 0 = never. */
     int32_t merge_run;
-    int32_t reserved;   /* must be 0 */
+    /* Threads per search CTA (no reference counterpart; results do not depend
+     * on it): 512 (two CTAs per SM) or 256 (four per SM); 0 = the geometry's
+     * default, 256 for ATB_GEOM_FIXED and 512 for ATB_GEOM_BINNED. */
+    int32_t cta_threads;
 } atb_params;
 
 /*
@@ -260,7 +263,8 @@ int atb_debug_fold(atb_handle* h, const atb_params* params, const double* t, con
  * ATB_STATIC_SCRATCH_BYTES large, that every GPU which loads the library holds
  * until the process exits.  Limits: at most ATB_STATIC_MAX_POINTS points, at
  * most 32 durations, and every period's bin count must fit the search kernel's
- * shared-memory histograms (larger ones are rejected; use the plan API).
+ * shared-memory histograms (larger ones are rejected; use the plan API).  The
+ * search runs 512-thread CTAs: params->cta_threads must be 0 or 512.
  * Errors are written to err (err_len bytes, may be NULL); no exception.  The
  * call itself allocates nothing on host or device: it calls no cudaMalloc,
  * cudaFree or allocating library routine.

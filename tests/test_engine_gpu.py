@@ -347,6 +347,10 @@ def test_edge_cases(engine):
     g = run(engine, t, f, None, [0.3], [0.05, 0.25, 0.5], cfg_binned())
     o = O.eng_binned(t, f, None, [0.3], [0.05, 0.25, 0.5])
     assert_bit_exact(g, o, "long-durations")
+    # a CTA size the library has no kernel for is an argument error
+    from astro_transit_gpu_b200.engine import SearchConfig
+    with pytest.raises(ValueError, match="cta_threads"):
+        run(engine, t, f, None, [0.3], [0.05], SearchConfig("parity", cta_threads=384))
 
 
 # -------------------------------------------------------- drop-in API ---
@@ -529,8 +533,8 @@ def test_tile_size_never_changes_results_and_autotune_picks_one(engine, tmp_path
     b = CurveBatch.from_arrays(list(t), list(y), list(dy), periods=per,
                                durations=R.C0_DURATIONS, device=engine.device)
     ref = None
-    for tp in (0, 1, 7, 8, 64):
-        cfg = SearchConfig("parity", objective="likelihood", tile_periods=tp)
+    for tp, nt in ((0, 0), (1, 256), (7, 512), (8, 256), (64, 0)):
+        cfg = SearchConfig("parity", objective="likelihood", tile_periods=tp, cta_threads=nt)
         out = {k: v.cpu().numpy() for k, v in engine.search(b, cfg).items()}
         if ref is None:
             ref = out
@@ -542,10 +546,12 @@ def test_tile_size_never_changes_results_and_autotune_picks_one(engine, tmp_path
     engine.tuning = TuningTable(str(tmp_path / "tuning.json"), saved.device_name,
                                 saved.library)
     try:
-        best = engine.autotune(b, cfg, candidates=(8, 64), fold_candidates=(0, 1, -1))
+        best = engine.autotune(b, cfg, candidates=(8, 64), fold_candidates=(0, 1, -1),
+                               shape_candidates=(512, 256))
         assert best["tile_periods"] in (8, 64)
         assert best["merge_run"] in (0, 1, -1)
-        assert len(engine.last_tune) == 5
+        assert best["cta_threads"] in (512, 256)
+        assert len(engine.last_tune) == 7
         key = engine.tune_key(b, cfg)
         assert engine.tuning.get(key)["tile_periods"] == best["tile_periods"]
         # persisted: a table read back from the file holds the same setting

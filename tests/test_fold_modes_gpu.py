@@ -1,6 +1,8 @@
 """The fold strategies (point by point, or a thread's points added once when
 they provably share a slot) are chosen per period from the expected points
-per bin; they only change how many shared-memory reductions are issued.  Every strategy, forced
+per bin; they only change how many shared-memory reductions are issued, and
+the CTA size (512 or 256 threads) only how the work is split.  Every
+strategy in both CTA sizes, forced
 on curves where it does and does not pay (dense and sparse, time-ordered and
 not, with gaps longer than the period, ragged lengths that leave warps
 partly empty, uniform and non-uniform weights), must give bit-identical
@@ -16,6 +18,8 @@ pytestmark = pytest.mark.gpu
 FIELDS = ("power", "depth", "depth_err", "t0", "duration", "window")
 # merge_run: the default; point by point only; merged wherever possible
 MODES = [0, -1, 1]
+# (merge_run, cta_threads): each fold mode in both CTA sizes
+SETTINGS = [(0, 0), (-1, 0), (1, 0), (0, 256), (1, 256), (-1, 512)]
 
 
 def _search(engine, t, y, w, periods, durs, cfg):
@@ -66,15 +70,15 @@ def test_every_fold_mode_is_bit_exact(engine, name, method):
         ora = O.eng_fixed(t, y, w, periods, durs, n_bins=200)
     else:
         ora = O.eng_binned(t, y, w, periods, durs, objective="likelihood")
-    for mr in MODES:
+    for mr, nt in SETTINGS:
         if method == "fast":
-            cfg = SearchConfig("fast", n_bins=200, merge_run=mr)
+            cfg = SearchConfig("fast", n_bins=200, merge_run=mr, cta_threads=nt)
         else:
-            cfg = SearchConfig("parity", objective="likelihood", merge_run=mr)
+            cfg = SearchConfig("parity", objective="likelihood", merge_run=mr, cta_threads=nt)
         g = _search(engine, t, y, w, periods, durs, cfg)
         for k in FIELDS:
             bad = np.flatnonzero(g[k] != ora[k])
-            assert bad.size == 0, (name, method, mr, k, bad[:5])
+            assert bad.size == 0, (name, method, mr, nt, k, bad[:5])
 
 
 def test_fold_modes_in_a_ragged_batch(engine):
@@ -92,9 +96,9 @@ def test_fold_modes_in_a_ragged_batch(engine):
         ps.append(per)
     b = CurveBatch.from_arrays(ts, ys, periods=ps, durations=R.C2_DURATIONS[:6])
     ref = None
-    for mr in MODES:
-        out = {k: v.cpu().numpy() for k, v in
-               engine.search(b, SearchConfig("fast", n_bins=200, merge_run=mr)).items()}
+    for mr, nt in SETTINGS:
+        cfg = SearchConfig("fast", n_bins=200, merge_run=mr, cta_threads=nt)
+        out = {k: v.cpu().numpy() for k, v in engine.search(b, cfg).items()}
         ref = ref or out
         for k in ref:
-            assert np.array_equal(out[k], ref[k]), (mr, k)
+            assert np.array_equal(out[k], ref[k]), (mr, nt, k)
