@@ -6,9 +6,11 @@
 //                  deterministic fixed-point staging q_w = rint(w*2^s_w),
 //                  q_y = rint(w*(y-c)*2^s_y) (|q| <= 2^27), per-curve totals,
 //                  the curve's histogram word layout (kPack*) and staged order.
-//   search kernel  persistent; CTAs pop (curve, period-chunk) tiles from a
-//                  device counter.  Periods of a tile are packed into groups
-//                  whose histograms fit shared memory; each thread keeps kR = 4
+//   search kernel  persistent; CTAs (512 threads, two per SM, or 256 threads,
+//                  four per SM, chosen per plan) pop (curve, period-chunk)
+//                  tiles from a device counter.  Periods of a tile are packed
+//                  into groups whose histograms fit shared memory; each
+//                  thread keeps kR = 4
 //                  time-ordered points in registers and folds them into every
 //                  period of the group (FP64 fold, identical to the reference's
 //                  per-point formula), adding each point's exact integer sums
