@@ -47,3 +47,31 @@ def test_structs_match_header_layout():
     assert ctypes.sizeof(N.Params) == 32
     assert ctypes.sizeof(N.Batch) == 8 + 12 * 8
     assert ctypes.sizeof(N.Outputs) == 8 * 8
+
+
+def test_params_field_offsets():
+    # the eight int32 fields of atb_params in header order
+    names = ["geometry", "objective", "n_bins", "oversample", "max_bins", "tile_periods",
+             "merge_run", "cta_threads"]
+    assert [f[0] for f in N.Params._fields_] == names
+    assert [getattr(N.Params, f).offset for f in names] == [4 * i for i in range(8)]
+
+
+def test_static_entry_validates_before_touching_the_device():
+    """Argument errors of the no-allocation entry point are found on the host
+    (no CUDA call is made): an unsupported CTA size and a bad point count.
+    The array arguments are host addresses that are never dereferenced."""
+    L = N.load()
+    dummy = (ctypes.c_double * 8)()
+    p = ctypes.cast(dummy, ctypes.c_void_p)
+    err = ctypes.create_string_buffer(256)
+
+    def call(prm, n=8):
+        return L.atb_search_curve_static(ctypes.byref(prm), p, p, 0, None, n, p, 2, p, 1, p,
+                                         None, None, None, None, None, None, None, err,
+                                         len(err))
+
+    prm = N.Params(N.GEOM_FIXED, N.OBJ_FAST, 200, 10, 0, 0, 0, 256)
+    assert call(prm) == N.ATB_EINVAL and b"cta_threads" in err.value
+    prm = N.Params(N.GEOM_FIXED, N.OBJ_FAST, 200, 10, 0, 0, 0, 0)
+    assert call(prm, n=N.STATIC_MAX_POINTS + 1) == N.ATB_EINVAL and b"points" in err.value
