@@ -74,6 +74,10 @@ constexpr int kR = ATB_POINTS_PER_THREAD;    // consecutive points a thread hold
 constexpr int kTileP = 64;             // periods per work-queue tile
 constexpr int kMaxG = 64;              // periods per shared-memory group
 constexpr int kMaxDur = 32;            // durations per curve
+// Window lengths in bins are clamped to kLenCap: every bin count is below 2^27,
+// so a clamped window never fits a period (it is skipped exactly as the
+// unclamped one) and start + length never overflows an int.
+constexpr int kLenCap = 1 << 28;
 constexpr int kStageAlign = 32;        // staged curves start at multiples of 32 points
 constexpr int kStageBlock = 256;
 constexpr double kDefaultMergeRun = 8.0;   // atb_params.merge_run = 0
@@ -590,10 +594,16 @@ __global__ void __launch_bounds__(kStageBlock) stage_kernel(const StageArgs a) {
         const double* dur = a.durations + a.dur_beg[c];
         double min_dur = dur[0];
         for (int k = 1; k < nd; ++k) min_dur = min(min_dur, dur[k]);
-        if (!(min_dur > 0.0) || !isfinite(min_dur)) atomicOr(a.status, 2);
+        bool bad_dur = !(min_dur > 0.0) || !isfinite(min_dur);
         const double bin_dur = min_dur / (double)a.oversample;
         const double ibd = 1.0 / bin_dur;
-        for (int k = 0; k < nd; ++k) a.dbins[c * kMaxDur + k] = (int)round(dur[k] * ibd);
+        for (int k = 0; k < nd; ++k) {
+            // a valid duration is >= min_dur, so its length is >= oversample >= 1
+            const double v = round(dur[k] * ibd);
+            bad_dur = bad_dur || !(dur[k] > 0.0) || !isfinite(dur[k]);
+            a.dbins[c * kMaxDur + k] = v >= (double)kLenCap ? kLenCap : (v >= 1.0 ? (int)v : 1);
+        }
+        if (bad_dur) atomicOr(a.status, 2);
         CurveStat st;
         st.t_start = t_start;
         st.shift = shift;
@@ -1448,9 +1458,9 @@ __device__ void finalize_period(const SearchArgs& a, GroupSmem& gs, const Team& 
         team_sync(tm);
     } else {
         if (tm.tid < nd) {
-            int L = (int)fma(gs.dur[tm.tid] * IP, (double)NB, 0.5);
-            if (L < 1) L = 1;
-            gs.L[tm.id][tm.tid] = L;
+            // truncation of dur/P * n_bins + 0.5, at least 1 (NaN: 1)
+            const double Lf = fma(gs.dur[tm.tid] * IP, (double)NB, 0.5);
+            gs.L[tm.id][tm.tid] = Lf >= (double)kLenCap ? kLenCap : (Lf >= 1.0 ? (int)Lf : 1);
         }
     }
     team_scan(tm, gs, E, NB + 1, st, cview);
@@ -3082,22 +3092,15 @@ extern "C" int atb_search_curve_static(const atb_params* prm, const double* t, c
     const long long n_tiles = (n_periods + kTileP - 1) / kTileP;
     static_meta_init<<<1, 32, 0, s>>>(m, n, n_periods, n_durations, n_tiles);
 
-    int nb_max = prm->n_bins;
-    if (prm->geometry == ATB_GEOM_BINNED) {
+    // fixed bins: one histogram of n_bins per period must fit shared memory
+    if (prm->geometry == ATB_GEOM_FIXED && prm->n_bins + 2 > cap)
+        return static_fail(err, err_len, ATB_EINVAL,
+                           "n_bins=%d; this entry point holds at most %d bins per period "
+                           "(use the plan API)", prm->n_bins, cap - 2);
+    if (prm->geometry == ATB_GEOM_BINNED)
         nbins_max_kernel<<<1, 256, 0, s>>>(1, m->per_beg, m->per_cnt, m->dur_beg, m->dur_cnt,
                                            periods, durations, prm->oversample, prm->max_bins,
                                            &m->nb_max);
-        e = cudaMemcpyAsync(&nb_max, &m->nb_max, sizeof(int), cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-        if (e != cudaSuccess)
-            return static_fail(err, err_len, ATB_ECUDA, "bin count: %s", cudaGetErrorString(e));
-    }
-    if (nb_max + 2 > cap)
-        return static_fail(err, err_len, ATB_EINVAL,
-                           "a period needs %d bins; this entry point holds at most %d per period "
-                           "(use the plan API)", nb_max, cap - 2);
-    if ((long long)nb_max * n_durations >= (1LL << 31))
-        return static_fail(err, err_len, ATB_EINVAL, "bins x durations too large");
 
     StageArgs sa{};
     sa.pt_off = m->pt_off;
@@ -3126,6 +3129,37 @@ extern "C" int atb_search_curve_static(const atb_params* prm, const double* t, c
         stage_kernel<double><<<1, kStageBlock, 0, s>>>(sa);
     else
         stage_kernel<float><<<1, kStageBlock, 0, s>>>(sa);
+
+    // Astropy bins: the largest period's bin count and the durations' window
+    // lengths in bins (written by the stage kernel).  A period whose
+    // histogram does not fit shared memory is searched in bin-range passes
+    // through shared memory when the search kernel takes that path for it
+    // (oversample <= kMpPadMax and a pass holds >= 64 window starts); the
+    // global-histogram path, which needs allocated memory, is rejected here.
+    int nb_max = prm->n_bins;
+    if (prm->geometry == ATB_GEOM_BINNED) {
+        int dbins[kMaxDur];
+        e = cudaMemcpyAsync(&nb_max, &m->nb_max, sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(dbins, m->dbins, sizeof(int) * n_durations,
+                                cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess)
+            return static_fail(err, err_len, ATB_ECUDA, "bin count: %s", cudaGetErrorString(e));
+        int lmax = 0;
+        for (int k = 0; k < n_durations; ++k) lmax = std::max(lmax, dbins[k]);
+        const bool passes = prm->oversample <= kMpPadMax && cap - 2 - lmax >= 64;
+        if (nb_max + 2 > cap && !passes)
+            return static_fail(err, err_len, ATB_EINVAL,
+                               "a period needs %d bins and windows of %d bins; this entry point "
+                               "holds at most %d per period (use the plan API)",
+                               nb_max, lmax, cap - 2);
+        if (nb_max >= (1 << 27))
+            return static_fail(err, err_len, ATB_EINVAL, "a period needs %d bins (limit 2^27)",
+                               nb_max);
+    }
+    if ((long long)nb_max * n_durations >= (1LL << 31))
+        return static_fail(err, err_len, ATB_EINVAL, "bins x durations too large");
 
     SearchArgs qa{};
     qa.objective = prm->objective;
@@ -3157,7 +3191,7 @@ extern "C" int atb_search_curve_static(const atb_params* prm, const double* t, c
     qa.t0 = t0;
     qa.duration = duration;
     qa.window = window;
-    qa.ghist = nullptr;  // never reached: every period fits shared memory (checked above)
+    qa.ghist = nullptr;  // never reached: oversized periods take the passes (checked above)
     qa.ghist_stride = 0;
     qa.tile_counter = &m->tile_counter;
     qa.tile_p = kTileP;

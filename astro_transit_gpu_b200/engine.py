@@ -173,6 +173,12 @@ class CurveBatch:
 
         per, pbeg, pcnt = grids(periods, "periods")
         dur, dbeg, dcnt = grids(durations, "durations")
+        # the kernels flag these too (ATB_EDATA); rejecting them here runs nothing
+        for name, arr in (("periods", per), ("durations", dur)):
+            if not np.all(np.isfinite(arr) & (arr > 0)):
+                raise ValueError(f"{name} must be positive and finite")
+        if np.any(dcnt < 1) or np.any(dcnt > 32):
+            raise ValueError("each curve needs 1 to 32 durations")
         obeg = np.zeros(nc, np.int64)
         np.cumsum(pcnt[:-1], out=obeg[1:])
 

@@ -97,3 +97,19 @@ def test_top_peak_indices_matches_find_peaks_without_ties():
         assert top_peak_indices(x, k, dist) == [int(i) for i in ref]
     # equal powers: the higher index first
     assert top_peak_indices(np.array([0, 2, 0, 2, 0.0]), 2, 1) == [3, 1]
+
+
+@pytest.mark.parametrize("periods, durations, msg", [
+    ([1.0, float("nan")], [0.1], "periods must be positive and finite"),
+    ([1.0, -2.0], [0.1], "periods must be positive and finite"),
+    ([1.0], [0.1, 0.0], "durations must be positive and finite"),
+    ([1.0], [float("inf")], "durations must be positive and finite"),
+    ([1.0], [], "durations must be positive|1 to 32 durations"),
+    ([1.0], list(np.linspace(0.01, 0.3, 33)), "1 to 32 durations"),
+])
+def test_curve_batch_rejects_invalid_grids_before_device_work(periods, durations, msg):
+    """Invalid grids are rejected on the host, before any copy or launch (the
+    kernels also flag them, as ATB_EDATA)."""
+    t, y, dy = _curve()
+    with pytest.raises(ValueError, match=msg):
+        CurveBatch.from_arrays([t], [y], periods=periods, durations=durations)

@@ -99,10 +99,36 @@ def test_static_entry_rejects_what_exceeds_its_scratch():
     t = np.linspace(0.0, 30.0, n)
     rc, msg, _ = call_static(t, np.ones(n, np.float32), None, [1.0, 2.0], [0.1], cfg)
     assert rc == N.ATB_EINVAL and "static scratch" in msg
-    # a period needing more bins than one shared-memory histogram holds
+    # periods needing more bins than one shared-memory histogram holds, where
+    # the search would need a global histogram: bins finer than the bin-range
+    # passes take (oversample > 16), windows too long for a pass, fixed bins
     t = np.linspace(0.0, 30.0, 1000)
-    rc, msg, _ = call_static(t, np.ones(1000, np.float32), None, [25.0], [0.001], cfg)
+    y = np.ones(1000, np.float32)
+    rc, msg, _ = call_static(t, y, None, [25.0], [0.01], SearchConfig("parity", oversample=20))
     assert rc == N.ATB_EINVAL and "bins" in msg
+    rc, msg, _ = call_static(t, y, None, [25.0], [0.002, 1.5], cfg)
+    assert rc == N.ATB_EINVAL and "bins" in msg
+    rc, msg, _ = call_static(t, y, None, [25.0], [0.1], SearchConfig("fast", n_bins=100000))
+    assert rc == N.ATB_EINVAL and "n_bins" in msg
+
+
+def test_static_entry_searches_long_periods_in_bin_range_passes():
+    """Astropy-binned periods whose bins do not fit one shared-memory
+    histogram (here up to 125 000 bins of 0.0002 d) are searched in bin-range
+    passes through shared memory, which need no allocated memory: the
+    outputs equal the plan API's, bit for bit."""
+    rng = np.random.default_rng(21)
+    t = np.sort(rng.uniform(1000.0, 1030.0, 6000))
+    y = R.inject_box(t, 1.0 + rng.normal(0, 1e-3, t.size), 11.3, 1003.0, 0.12, 5e-3)
+    y32 = y.astype(np.float32)
+    w = (1.0 / (1e-3 * (1.0 + rng.uniform(size=t.size))) ** 2).astype(np.float32)
+    periods = np.concatenate([np.linspace(0.9, 3.0, 40), np.geomspace(10.0, 25.0, 24)])
+    durs = [0.002, 0.01, 0.05, 0.12]
+    for cfg in (SearchConfig("parity", objective="likelihood"),
+                SearchConfig("parity", objective="snr", max_bins=0)):
+        rc, msg, got = call_static(t, y32, w, periods, durs, cfg)
+        assert rc == N.ATB_OK, msg
+        assert_same(got, call_plan(t, y32, w, periods, durs, cfg), cfg.objective)
 
 
 def test_static_entry_recovers_from_invalid_data_and_runs_without_best_index():
