@@ -262,8 +262,12 @@ int atb_debug_fold(atb_handle* h, const atb_params* params, const double* t, con
  * NULL).  All other working memory is one array built into the library,
  * ATB_STATIC_SCRATCH_BYTES large, that every GPU which loads the library holds
  * until the process exits.  Limits: at most ATB_STATIC_MAX_POINTS points, at
- * most 32 durations, and every period's bin count must fit the search kernel's
- * shared-memory histograms (larger ones are rejected; use the plan API).  The
+ * most 32 durations, and a period whose bins do not fit one shared-memory
+ * histogram is accepted only where the search takes it in bin-range passes
+ * through shared memory (astropy-binned geometry, oversample <= 16, the
+ * longest window at least 64 bins shorter than a pass); others -- fixed bins
+ * beyond the histogram, finer or longer-windowed astropy bins -- would need a
+ * global histogram and are rejected (use the plan API).  The
  * search runs 512-thread CTAs: params->cta_threads must be 0 or 512.
  * Errors are written to err (err_len bytes, may be NULL); no exception.  The
  * call itself allocates nothing on host or device: it calls no cudaMalloc,
