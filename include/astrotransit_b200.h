@@ -19,7 +19,8 @@
  *     above; its Python counterpart is astro_transit_gpu_b200.api.
  * The reference has no native FFI of its own (CuPy JIT-compiles the kernels
  * at run time, gpu_bls.py:18-40, v42_parity.py:7-25); these entry points are
- * what a maintainer binds instead.
+ * what a maintainer binds instead, with ctypes (the single-call entry points
+ * take the same arrays the CuPy launches take).
  */
 #ifndef ASTROTRANSIT_B200_H
 #define ASTROTRANSIT_B200_H

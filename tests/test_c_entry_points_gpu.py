@@ -1,7 +1,7 @@
 """The two single-call C entry points a maintainer binds into the reference,
-called through ctypes exactly as INTEGRATION.md's stubs bind them (the
-stubs take CuPy arrays; torch tensors stand in here, the pointers are the
-same kind):
+called through ctypes exactly as the reference-side ctypes stubs bind them
+(the stubs take CuPy arrays; torch tensors stand in here, the pointers are
+the same kind):
 
 * atb_run_gpu_bls            run_gpu_bls + bls_kernel (search/gpu_bls.py:42-144)
 * atb_run_vbls_exact_parity  run_vbls_exact_parity + vbls_v42_parity_kernel
@@ -29,7 +29,7 @@ POWER_RTOL = 1e-5  # relative power error bound against the FP64 oracle
 
 
 def stub_library():
-    """The library bound the way INTEGRATION.md's ctypes stubs bind it."""
+    """The library bound the way the reference-side ctypes stubs bind it."""
     c = ctypes
     lib = c.CDLL(N.lib_path())
     lib.atb_create.argtypes = [c.c_int, c.POINTER(c.c_void_p)]
