@@ -1,8 +1,8 @@
 /*
  * bls_oracle.c -- CPU restatement of the reference's Box Least Squares hot path.
  *
- * TEST INFRASTRUCTURE ONLY.  This file is the checker for the CUDA engine in
- * astro_transit_gpu_b200/csrc.  Only the test-suite, the smoke check and the
+ * TEST INFRASTRUCTURE ONLY.  This file is the oracle the tests compare the
+ * CUDA engine in astro_transit_gpu_b200/csrc against.  Only the test-suite, the smoke check and the
  * CPU-baseline leg of bench.py load it; the product path never does.
  *
  * Two families of functions live here.

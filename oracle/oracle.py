@@ -1,6 +1,6 @@
 """ctypes wrapper of the FP64 CPU oracle (``bls_oracle.c``).
 
-TEST INFRASTRUCTURE ONLY: the checker for the CUDA engine.  Imported by the
+TEST INFRASTRUCTURE ONLY: the oracle the CUDA engine is tested against.  Imported by the
 test-suite, by ``__graft_entry__.smoke()`` and by the CPU-baseline leg of
 ``bench.py``; never by the product package.
 
