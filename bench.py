@@ -212,7 +212,7 @@ def make_workload(args, rank, world):
         dy = np.stack([c[2] for c in cs])
         return {"t": np.stack([c[0] for c in cs]), "y": np.stack([c[1] for c in cs]),
                 "dy": dy, "w": weights(dy), "periods": R.precision_periods(),
-                "durations": list(R.C3_DURATIONS)}
+                "durations": list(R.PRECISION_DURATIONS)}
     if args.workload == "mixed":
         total = args.curves * world
         specs = [R.mixed_spec_indexed(2000, i) for i in range(total)]
@@ -221,9 +221,9 @@ def make_workload(args, rank, world):
         cs = [R.mixed_curve_indexed(2000, int(i)) for i in mine]
         return {"t": [c[0] for c in cs], "y": [c[1] for c in cs], "dy": [c[2] for c in cs],
                 "w": [weights(c[2]) for c in cs], "periods": [c[3] for c in cs],
-                "durations": list(R.C2_DURATIONS)}
+                "durations": list(R.MIXED_DURATIONS)}
     t, y, dy, _ = R.uniform_batch(n_curves=args.curves, n=args.points, seed=1000 + rank)
-    return {"t": t, "y": y, "dy": dy, "w": weights(dy), "periods": R.c0_periods(args.periods),
+    return {"t": t, "y": y, "dy": dy, "w": weights(dy), "periods": R.sector_periods(args.periods),
             "durations": DURATIONS}
 
 
@@ -354,7 +354,7 @@ def serving_pool(n, seed=4000):
         n_sec, cad, npts, n_per = R.mixed_curve_spec(rng)
         t, y, dy, per = R.mixed_curve(rng, n_sec, cad, npts, n_per)
         pool.append(dict(t=t, y=y, dy=dy, periods=per,
-                         durations=R.C2_DURATIONS[:4 + int(rng.integers(0, 5))], method="fast"))
+                         durations=R.MIXED_DURATIONS[:4 + int(rng.integers(0, 5))], method="fast"))
     return pool
 
 

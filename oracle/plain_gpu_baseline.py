@@ -69,7 +69,7 @@ def main():
 
     nc = max(args.curves, args.sample)
     t, y, dy, _ = R.uniform_batch(n_curves=nc, n=15000, seed=1000)
-    periods = R.c0_periods(5000)
+    periods = R.sector_periods(5000)
     rk = RefKernels()
     out = {"workload": "uniform batch curves: 15000 points, 5000 log-spaced periods 0.5-13.7 d, "
                        "6 durations 0.04-0.20 d", "sample_curves": args.sample}
@@ -123,7 +123,7 @@ def mixed(args):
     sample are scaled by the sample's share of the batch's fold updates so
     that both rates refer to the same curve-size distribution."""
     cs = R.mixed_batch(args.curves, seed=2000)
-    durs = R.C2_DURATIONS
+    durs = R.MIXED_DURATIONS
     rk = RefKernels()
     rng = np.random.default_rng(0)
     idx = np.sort(rng.choice(len(cs), size=min(args.sample, len(cs)), replace=False))

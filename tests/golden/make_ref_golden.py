@@ -21,9 +21,9 @@ import recipes as R  # noqa: E402
 from oracle.ref_kernels import RefKernels  # noqa: E402
 
 
-def c0_small(n=3000, n_periods=400, seed=7):
-    t, y, dy = R.c0_curve(n=n, seed=seed)
-    return t, y, dy, R.c0_periods(n_periods), R.C0_DURATIONS
+def sector_small(n=3000, n_periods=400, seed=7):
+    t, y, dy = R.sector_curve(n=n, seed=seed)
+    return t, y, dy, R.sector_periods(n_periods), R.SECTOR_DURATIONS
 
 
 def fast_weighted(seed=11):
@@ -51,8 +51,8 @@ def main():
     v42_cases = {
         "v42_test": (R.v42_test_recipe(), 4000),
         "v42_debug": (R.v42_debug_recipe(), 2000),
-        "v42_c0small": (c0_small(), 3600),
-        "v42_cap": (c0_small(), 2000),  # reference default cap active for P > 7.96 d
+        "v42_c0small": (sector_small(), 3600),
+        "v42_cap": (sector_small(), 2000),  # reference default cap active for P > 7.96 d
     }
     for name, ((t, y, dy, periods, durs), max_bins) in v42_cases.items():
         w = 1.0 / dy ** 2
@@ -87,9 +87,9 @@ def main():
     fast_cases = {
         "bls_astropy_test": (R.astropy_parity_recipe(), 500),
         "bls_recovery": (R.recovery_recipe(), 200),
-        "bls_c0small": (c0_small(), 200),
+        "bls_c0small": (sector_small(), 200),
         "bls_weighted_unsorted": (fast_weighted(), 300),
-        "bls_nbins1024": (c0_small(n=2000, n_periods=200, seed=3), 1024),
+        "bls_nbins1024": (sector_small(n=2000, n_periods=200, seed=3), 1024),
     }
     for name, ((t, y, dy, periods, durs), nb) in fast_cases.items():
         r64 = rk.run_gpu_bls(t, y, periods, durs, flux_err=dy, n_bins=nb, dtype=np.float64)

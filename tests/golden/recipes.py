@@ -65,10 +65,10 @@ def recovery_recipe():
 
 
 SECTOR_DAYS = 27.4
-C0_DURATIONS = np.array([0.04, 0.06, 0.08, 0.12, 0.16, 0.20])
+SECTOR_DURATIONS = np.array([0.04, 0.06, 0.08, 0.12, 0.16, 0.20])
 
 
-def c0_periods(n=5000, pmin=0.5, pmax=13.7):
+def sector_periods(n=5000, pmin=0.5, pmax=13.7):
     """Log-spaced period grid of the single-curve workload."""
     return np.geomspace(pmin, pmax, n)
 
@@ -84,7 +84,7 @@ def sector_times(rng, n, t_offset=1325.0, gap=1.0):
     return t_offset + np.sort(out[:n])
 
 
-def c0_curve(n=15000, seed=0):
+def sector_curve(n=15000, seed=0):
     """Single-curve workload: N points over a sector with a 1 d mid-sector gap,
     y = 1 + N(0, 1e-3) with a box transit P=3.71, t0=1326.2, dur=0.10,
     depth=1.5e-3, dy = 1e-3."""
@@ -140,7 +140,7 @@ def uniform_batch(n_curves=4096, n=15000, seed=1, transit_fraction=0.3):
     return t, y, dy, truth
 
 
-C2_DURATIONS = np.geomspace(0.02, 0.3, 8)
+MIXED_DURATIONS = np.geomspace(0.02, 0.3, 8)
 
 
 def mixed_curve_spec(rng):
@@ -218,7 +218,7 @@ def precision_periods(n=100_000, pmin=0.5, pmax=150.0):
     return 1.0 / np.linspace(1.0 / pmin, 1.0 / pmax, n)[::-1]
 
 
-C3_DURATIONS = np.geomspace(0.02, 0.3, 8)
+PRECISION_DURATIONS = np.geomspace(0.02, 0.3, 8)
 
 
 def mixed_spec_indexed(seed, i):

@@ -117,14 +117,14 @@ def assert_fields_equal(got, ora, fields, name):
 
 
 def test_run_gpu_bls_entry_point_weighted(stub):
-    t, y, dy = R.c0_curve(n=6000, seed=31)
+    t, y, dy = R.sector_curve(n=6000, seed=31)
     y = y.astype(np.float32)
-    periods = R.c0_periods(800)
-    got, best = call_run_gpu_bls(stub, t, y, dy, periods, R.C0_DURATIONS, 200)
+    periods = R.sector_periods(800)
+    got, best = call_run_gpu_bls(stub, t, y, dy, periods, R.SECTOR_DURATIONS, 200)
     w = (1.0 / dy.astype(np.float64) ** 2).astype(np.float32)
-    o = O.eng_fixed(t, y, w, periods, R.C0_DURATIONS, n_bins=200)
+    o = O.eng_fixed(t, y, w, periods, R.SECTOR_DURATIONS, n_bins=200)
     assert_fields_equal(got, o, ("power", "t0", "duration", "depth"), "run_gpu_bls")
-    a = O.ref_fixed(t, y, 1.0 / dy.astype(np.float64) ** 2, periods, R.C0_DURATIONS, n_bins=200)
+    a = O.ref_fixed(t, y, 1.0 / dy.astype(np.float64) ** 2, periods, R.SECTOR_DURATIONS, n_bins=200)
     rel = np.abs(got["power"] - a["power"]) / a["power"]
     assert rel.max() <= POWER_RTOL, rel.max()
     # the best index is the first maximum (gpu_bls.py:131, cupy.argmax)
@@ -153,14 +153,14 @@ def test_run_vbls_exact_parity_entry_point_multi_target(stub, max_bins, objectiv
     ys = np.stack([R.inject_box(t, 1.0 + rng.normal(0, 1e-3, t.size), P, t[0] + 0.3 * k,
                                 0.12, 2.5e-3) for k, P in enumerate(truth)]).astype(np.float32)
     ws = (1.0 / (1e-3 * (1.0 + 0.5 * rng.uniform(size=ys.shape))) ** 2).astype(np.float32)
-    periods = R.c0_periods(700)
-    got, best = call_run_vbls(stub, t, ys, ws, periods, R.C0_DURATIONS, 10, max_bins, objective)
+    periods = R.sector_periods(700)
+    got, best = call_run_vbls(stub, t, ys, ws, periods, R.SECTOR_DURATIONS, 10, max_bins, objective)
     for k in range(len(truth)):
         gk = {f: v[k] for f, v in got.items()}
-        o = O.eng_binned(t, ys[k], ws[k], periods, R.C0_DURATIONS, max_bins=max_bins,
+        o = O.eng_binned(t, ys[k], ws[k], periods, R.SECTOR_DURATIONS, max_bins=max_bins,
                          objective=objective)
         assert_fields_equal(gk, o, ("power", "t0", "duration", "depth"), f"target {k}")
-        a = O.ref_binned(t, ys[k], ws[k].astype(np.float64), periods, R.C0_DURATIONS,
+        a = O.ref_binned(t, ys[k], ws[k].astype(np.float64), periods, R.SECTOR_DURATIONS,
                          max_bins=max_bins, objective=objective)
         ok = a["power"] > 0
         rel = np.abs(gk["power"][ok] - a["power"][ok]) / a["power"][ok]

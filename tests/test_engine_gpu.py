@@ -61,17 +61,17 @@ def weighted_unsorted(n=3000, seed=9):
 
 def test_fold_slots_bit_exact(engine):
     """Per-point bin indices (V42 slots and fixed-bin slots) equal the FP64 fold."""
-    t, y, dy = R.c0_curve(n=5000, seed=1)
+    t, y, dy = R.sector_curve(n=5000, seed=1)
     w = (1 / dy ** 2).astype(np.float32)
-    periods = np.concatenate([R.c0_periods(300), [3.71, 0.5, 13.7, 1.0, 2.0, 4.0]])
+    periods = np.concatenate([R.sector_periods(300), [3.71, 0.5, 13.7, 1.0, 2.0, 4.0]])
     dev = engine.device
     tt = torch.tensor(t, device=dev)
     yy = torch.tensor(y.astype(np.float32), device=dev)
     ww = torch.tensor(w, device=dev)
     pp = torch.tensor(periods, device=dev)
-    dd = torch.tensor(R.C0_DURATIONS, device=dev)
+    dd = torch.tensor(R.SECTOR_DURATIONS, device=dev)
     slots = engine.debug_fold(tt, yy, ww, pp, dd, cfg_binned()).cpu().numpy()
-    ora = O.eng_binned(t, y.astype(np.float32), w, periods, R.C0_DURATIONS, point_bins=True)
+    ora = O.eng_binned(t, y.astype(np.float32), w, periods, R.SECTOR_DURATIONS, point_bins=True)
     assert np.array_equal(slots, ora["point_bins"])
     # counts per bin follow from the indices
     for p in (0, 150, 305):
@@ -79,7 +79,7 @@ def test_fold_slots_bit_exact(engine):
         assert np.array_equal(np.bincount(slots[p], minlength=nb),
                               np.bincount(ora["point_bins"][p], minlength=nb))
     slots = engine.debug_fold(tt, yy, ww, pp, dd, cfg_fixed(200)).cpu().numpy()
-    ora = O.eng_fixed(t, y.astype(np.float32), w, periods, R.C0_DURATIONS, n_bins=200,
+    ora = O.eng_fixed(t, y.astype(np.float32), w, periods, R.SECTOR_DURATIONS, n_bins=200,
                       point_bins=True)
     ora_slots = np.where(ora["point_bins"] < 0, 201, ora["point_bins"])
     assert np.array_equal(slots, ora_slots)
@@ -94,7 +94,7 @@ def test_fold_slots_bit_exact_precision_sample(engine):
     t, y, dy, _ = R.precision_curve(rng)
     w = (1 / dy.astype(np.float64) ** 2).astype(np.float32)
     periods = R.precision_periods()[::2000]
-    durs = R.C3_DURATIONS
+    durs = R.PRECISION_DURATIONS
     dev = engine.device
     slots = engine.debug_fold(torch.tensor(t, device=dev), torch.tensor(y, device=dev),
                               torch.tensor(w, device=dev), torch.tensor(periods, device=dev),
@@ -165,14 +165,14 @@ def test_binned_bit_exact_reference_recipe(engine, objective):
     assert_bit_exact(g, o, objective)
 
 
-def test_binned_bit_exact_c0_float32(engine):
-    t, y, dy = R.c0_curve(n=15000, seed=0)
+def test_binned_bit_exact_sector_float32(engine):
+    t, y, dy = R.sector_curve(n=15000, seed=0)
     y32 = y.astype(np.float32)
     w = (1 / dy ** 2).astype(np.float32)
-    periods = R.c0_periods(1000)
-    g = run(engine, t, y32, w, periods, R.C0_DURATIONS, cfg_binned("likelihood"))
-    o = O.eng_binned(t, y32, w, periods, R.C0_DURATIONS, objective="likelihood")
-    assert_bit_exact(g, o, "c0")
+    periods = R.sector_periods(1000)
+    g = run(engine, t, y32, w, periods, R.SECTOR_DURATIONS, cfg_binned("likelihood"))
+    o = O.eng_binned(t, y32, w, periods, R.SECTOR_DURATIONS, objective="likelihood")
+    assert_bit_exact(g, o, "sector")
 
 
 @pytest.mark.parametrize("n", [1, 7, 9, 4095, 5003])
@@ -200,11 +200,11 @@ def test_binned_bit_exact_weighted_unsorted(engine):
 
 
 def test_binned_bit_exact_reference_cap(engine):
-    t, y, dy = R.c0_curve(n=3000, seed=7)
+    t, y, dy = R.sector_curve(n=3000, seed=7)
     w = (1 / dy ** 2).astype(np.float32)
-    periods = R.c0_periods(400)
-    g = run(engine, t, y, w, periods, R.C0_DURATIONS, cfg_binned(max_bins=2000))
-    o = O.eng_binned(t, y, w, periods, R.C0_DURATIONS, max_bins=2000)
+    periods = R.sector_periods(400)
+    g = run(engine, t, y, w, periods, R.SECTOR_DURATIONS, cfg_binned(max_bins=2000))
+    o = O.eng_binned(t, y, w, periods, R.SECTOR_DURATIONS, max_bins=2000)
     assert_bit_exact(g, o, "cap")
 
 
@@ -269,13 +269,13 @@ def test_fixed_bit_exact_weighted_unsorted(engine):
 # ------------------------------------------------ tolerance vs FP64 ref ---
 
 def test_power_within_tolerance_of_fp64_reference(engine):
-    t, y, dy = R.c0_curve(n=15000, seed=0)
-    periods = R.c0_periods(2000)
+    t, y, dy = R.sector_curve(n=15000, seed=0)
+    periods = R.sector_periods(2000)
     w64 = 1 / dy ** 2
     for objective in ("snr", "likelihood"):
-        g = run(engine, t, y, w64.astype(np.float32), periods, R.C0_DURATIONS,
+        g = run(engine, t, y, w64.astype(np.float32), periods, R.SECTOR_DURATIONS,
                 cfg_binned(objective))
-        a = O.ref_binned(t, y, w64, periods, R.C0_DURATIONS, objective=objective)
+        a = O.ref_binned(t, y, w64, periods, R.SECTOR_DURATIONS, objective=objective)
         rel = np.abs(g["power"] - a["power"]) / a["power"]
         assert rel.max() <= POWER_RTOL, rel.max()
         assert np.argmax(g["power"]) == np.argmax(a["power"])
@@ -320,11 +320,11 @@ def test_ragged_batch_equals_single_curve_runs(engine):
 
 
 def test_results_are_bit_deterministic(engine):
-    t, y, dy = R.c0_curve(n=8000, seed=4)
+    t, y, dy = R.sector_curve(n=8000, seed=4)
     w = (1 / dy ** 2).astype(np.float32)
-    periods = R.c0_periods(1500)
-    a = run(engine, t, y, w, periods, R.C0_DURATIONS, cfg_binned())
-    b = run(engine, t, y, w, periods, R.C0_DURATIONS, cfg_binned())
+    periods = R.sector_periods(1500)
+    a = run(engine, t, y, w, periods, R.SECTOR_DURATIONS, cfg_binned())
+    b = run(engine, t, y, w, periods, R.SECTOR_DURATIONS, cfg_binned())
     assert_bit_exact(a, b, "rerun")
 
 
@@ -424,7 +424,7 @@ def test_batch_session_graph_replay_matches_eager(engine):
     from astro_transit_gpu_b200.engine import BatchSession, SearchConfig
     t, y, dy, _ = R.uniform_batch(n_curves=6, n=3000, seed=5)
     w = (1 / dy.astype(np.float64) ** 2).astype(np.float32)
-    periods, durs = R.c0_periods(400), R.C0_DURATIONS
+    periods, durs = R.sector_periods(400), R.SECTOR_DURATIONS
     pt = np.arange(7, dtype=np.int64) * 3000
     cfg = SearchConfig("parity", objective="likelihood")
     eager = BatchSession(engine, pt, periods, durs, cfg, weighted=True)
@@ -471,7 +471,7 @@ def test_pipelined_session_equals_one_session(engine, graphs):
     pt = np.zeros(8, np.int64)
     np.cumsum([len(a) for a in t], out=pt[1:])
     per = [p[:: max(1, len(p) // 700)] for p in per]
-    durs = list(R.C2_DURATIONS)
+    durs = list(R.MIXED_DURATIONS)
     cfg = SearchConfig("parity", objective="likelihood")
     one = BatchSession(engine, pt, per, durs, cfg)
     one.load(np.concatenate(t), np.concatenate(y), np.concatenate(w))
@@ -508,7 +508,7 @@ def test_screen_equals_full_search_at_its_best_period(engine, method):
         ts.append(t); ys.append(1.0 + y); es.append(dy); ps.append(per)
     cfg = (SearchConfig("fast", n_bins=128) if method == "fast" else
            SearchConfig("parity", objective="likelihood"))
-    b = CurveBatch.from_arrays(ts, ys, es, periods=ps, durations=R.C2_DURATIONS[:6],
+    b = CurveBatch.from_arrays(ts, ys, es, periods=ps, durations=R.MIXED_DURATIONS[:6],
                                device=engine.device)
     full = {k: v.cpu().numpy() for k, v in engine.search(b, cfg).items()}
     scr = {k: v.cpu().numpy() for k, v in engine.screen(b, cfg).items()}
@@ -531,7 +531,7 @@ def test_tile_size_never_changes_results_and_autotune_picks_one(engine, tmp_path
     t, y, dy, _ = R.uniform_batch(n_curves=3, n=3000, seed=17)
     per = [np.geomspace(0.5, 13.7, n) for n in (700, 1500, 333)]
     b = CurveBatch.from_arrays(list(t), list(y), list(dy), periods=per,
-                               durations=R.C0_DURATIONS, device=engine.device)
+                               durations=R.SECTOR_DURATIONS, device=engine.device)
     ref = None
     for tp, nt in ((0, 0), (1, 256), (7, 512), (8, 256), (64, 0)):
         cfg = SearchConfig("parity", objective="likelihood", tile_periods=tp, cta_threads=nt)

@@ -94,7 +94,7 @@ def test_fold_modes_in_a_ragged_batch(engine):
         ts.append(t)
         ys.append(y)
         ps.append(per)
-    b = CurveBatch.from_arrays(ts, ys, periods=ps, durations=R.C2_DURATIONS[:6])
+    b = CurveBatch.from_arrays(ts, ys, periods=ps, durations=R.MIXED_DURATIONS[:6])
     ref = None
     for mr, nt in SETTINGS:
         cfg = SearchConfig("fast", n_bins=200, merge_run=mr, cta_threads=nt)

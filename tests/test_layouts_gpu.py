@@ -94,11 +94,11 @@ def clustered(n_clusters=40, per_cluster=60, span=27.0, seed=3):
 
 CASES = {
     # name: (t, y, w, periods, durations, kind, n_bins, expected layout)
-    "c0_uniform": lambda: (*R.c0_curve(n=15000, seed=2)[:2], None, R.c0_periods(600),
-                           R.C0_DURATIONS, "binned", None, TIGHT),
+    "sector_uniform": lambda: (*R.sector_curve(n=15000, seed=2)[:2], None, R.sector_periods(600),
+                           R.SECTOR_DURATIONS, "binned", None, TIGHT),
     # fixed 200 bins: bound 3819 points, 12 bits (the largest tight layout)
-    "c0_uniform_fixed": lambda: (*R.c0_curve(n=15000, seed=2)[:2], None, R.c0_periods(600),
-                                 R.C0_DURATIONS, "fixed", 200, TIGHT),
+    "sector_uniform_fixed": lambda: (*R.sector_curve(n=15000, seed=2)[:2], None, R.sector_periods(600),
+                                 R.SECTOR_DURATIONS, "fixed", 200, TIGHT),
     # bursts of 60 simultaneous samples: bound 3300 points, bins reach 60+
     "clustered": lambda: (*clustered(seed=3), None, np.geomspace(0.5, 13.7, 500),
                           np.array([0.04, 0.1]), "binned", None, TIGHT),
@@ -106,8 +106,8 @@ CASES = {
                                 np.array([0.04, 0.1]), "fixed", 2000, TIGHT),
     # the reference's default cap (max_bins=2000) where no period reaches it:
     # 0.004 d bins up to 7.9 d need at most 1985 bins
-    "c0_uniform_cap_not_reached": lambda: (*R.c0_curve(n=15000, seed=2)[:2], None,
-                                           R.c0_periods(600, pmax=7.9), R.C0_DURATIONS,
+    "sector_uniform_cap_not_reached": lambda: (*R.sector_curve(n=15000, seed=2)[:2], None,
+                                           R.sector_periods(600, pmax=7.9), R.SECTOR_DURATIONS,
                                            "binned", 2000, TIGHT),
 }
 
@@ -137,13 +137,13 @@ def test_layout_falls_back_when_no_bound(engine):
     cases = [
         (t, y, None, "binned", None, CHECKED),
         # unsorted times: no bound is computed
-        (rng.permutation(R.c0_curve(n=4000, seed=4)[0]), rng.normal(1, 1e-3, 4000), None,
+        (rng.permutation(R.sector_curve(n=4000, seed=4)[0]), rng.normal(1, 1e-3, 4000), None,
          "binned", None, CHECKED),
         (t, y, None, "fixed", None, CHECKED),
         # a bin cap that the grid reaches folds many points into the last bin
-        (*R.c0_curve(n=4000, seed=4)[:2], None, "binned", 500, COUNT),
+        (*R.sector_curve(n=4000, seed=4)[:2], None, "binned", 500, COUNT),
         # non-uniform weights
-        (*R.c0_curve(n=4000, seed=4)[:2], rng.uniform(1e5, 2e5, 4000).astype(np.float32),
+        (*R.sector_curve(n=4000, seed=4)[:2], rng.uniform(1e5, 2e5, 4000).astype(np.float32),
          "binned", None, SPLIT),
     ]
     for t_, y_, w_, kind, mb, expect in cases:
@@ -179,7 +179,7 @@ def test_checked_tight_layout_refolds_overflowing_periods(engine, kind):
         assert np.array_equal(np.asarray(g[k]), np.asarray(o[k])), k
     assert max_occupancy(engine, t, y, None, periods, durs, cfg) >= 4096
     # in a batch with curves that pass the check
-    t2, y2 = R.c0_curve(n=9000, seed=13)[:2]
+    t2, y2 = R.sector_curve(n=9000, seed=13)[:2]
     b = CurveBatch.from_arrays([t2, t, t2], [y2.astype(np.float32), y, y2.astype(np.float32)],
                                periods=periods, durations=durs)
     outs = split_outputs(b, engine.search(b, cfg))

@@ -161,7 +161,7 @@ def test_injection_recovered_by_oracle():
 
 # --------------------------------------------------- engine arithmetic ---
 
-@pytest.mark.parametrize("recipe", ["v42_test", "c0", "weighted"])
+@pytest.mark.parametrize("recipe", ["v42_test", "sector", "weighted"])
 @pytest.mark.parametrize("objective", ["snr", "likelihood"])
 def test_engine_mirror_close_to_fp64_binned(recipe, objective):
     """The engine's arithmetic (fixed-point sums, FP32 search, FP64 winner) stays
@@ -169,9 +169,9 @@ def test_engine_mirror_close_to_fp64_binned(recipe, objective):
     wherever the FP64 runner-up is more than 1e-5 behind."""
     if recipe == "v42_test":
         t, y, dy, periods, durs = R.v42_test_recipe()
-    elif recipe == "c0":
-        t, y, dy = R.c0_curve(n=4000, seed=3)
-        periods, durs = R.c0_periods(600), R.C0_DURATIONS
+    elif recipe == "sector":
+        t, y, dy = R.sector_curve(n=4000, seed=3)
+        periods, durs = R.sector_periods(600), R.SECTOR_DURATIONS
     else:
         rng = np.random.default_rng(9)
         t = np.sort(rng.uniform(100.0, 140.0, 3000))
@@ -198,7 +198,7 @@ def test_engine_mirror_close_to_fp64_fixed():
 
 def test_engine_stage_is_order_independent():
     """The fixed-point staging (shift, scales, totals) does not depend on point order."""
-    t, y, dy = R.c0_curve(n=2000, seed=5)
+    t, y, dy = R.sector_curve(n=2000, seed=5)
     w = (1 / dy ** 2).astype(np.float32)
     perm = np.random.default_rng(0).permutation(t.size)
     _, qw, qy, st = O.eng_stage(t, y, w)
@@ -212,9 +212,9 @@ def test_engine_stage_is_order_independent():
 
 def test_cap_reproduces_reference_pileup():
     """max_bins caps n_bins at max_bins-1 and clamps indices (vbls_v42_parity.cu:46-47,70)."""
-    t, y, dy = R.c0_curve(n=1500, seed=2)
+    t, y, dy = R.sector_curve(n=1500, seed=2)
     periods = np.array([5.0, 9.0, 12.0])
-    o = O.eng_binned(t, y, (1 / dy ** 2).astype(np.float32), periods, R.C0_DURATIONS,
+    o = O.eng_binned(t, y, (1 / dy ** 2).astype(np.float32), periods, R.SECTOR_DURATIONS,
                      max_bins=2000, point_bins=True)
     pb = o["point_bins"]
     assert pb[0].max() <= 1260  # ceil(5/0.004) = 1250 real bins, uncapped

@@ -18,7 +18,7 @@ def _requests(n=12, seed=4):
         n_sec, cad, npts, nper = R.mixed_curve_spec(rng)
         t, y, dy, per = R.mixed_curve(rng, n_sec, cad, min(npts, 6000), min(nper, 1500))
         method = "fast" if i % 3 == 0 else "parity"
-        durs = R.C2_DURATIONS[: 4 + i % 5]
+        durs = R.MIXED_DURATIONS[: 4 + i % 5]
         reqs.append(dict(t=t, y=y, dy=dy, periods=per, durations=durs, method=method,
                          objective=None if method == "fast" else "likelihood"))
     return reqs
@@ -77,7 +77,7 @@ def test_timeout_and_cancellation_before_admission(engine):
     big_t, big_y, big_dy, big_p = R.mixed_curve(rng, 13, R.CADENCE_2MIN, 150000, 40000)
     small = _requests(n=2, seed=23)
     with BLSServer(max_batch=1, n_streams=1) as srv:
-        f_big = srv.submit(big_t, big_y, big_dy, periods=big_p, durations=R.C2_DURATIONS)
+        f_big = srv.submit(big_t, big_y, big_dy, periods=big_p, durations=R.MIXED_DURATIONS)
         f_exp = srv.submit(**small[0], timeout=1e-6)
         f_can = srv.submit(**small[0])
         cancelled = f_can.cancel()

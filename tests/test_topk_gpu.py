@@ -21,7 +21,7 @@ def _plan(engine, n_curves, n_periods):
     t, y, dy, _ = R.uniform_batch(n_curves=n_curves, n=2000, seed=8)
     per = [np.geomspace(0.5, 10.0, n) for n in n_periods]
     b = CurveBatch.from_arrays(list(t), list(y), list(dy), periods=per,
-                               durations=R.C0_DURATIONS, device=engine.device)
+                               durations=R.SECTOR_DURATIONS, device=engine.device)
     plan = engine.plan(b, SearchConfig("fast", n_bins=200))
     plan.execute()
     torch.cuda.synchronize()
@@ -77,7 +77,7 @@ def test_power_batch_equals_single_calls_with_device_peaks(engine):
         n_sec, cad, n, n_per = R.mixed_curve_spec(rng)
         t, y, dy, per = R.mixed_curve(rng, n_sec, cad, min(n, 5000), min(n_per, 2000))
         curves.append((t, 1.0 + y, dy, per))
-    durs = R.C2_DURATIONS[:5]
+    durs = R.MIXED_DURATIONS[:5]
     for method in ("fast", "parity"):
         batch = power_batch([c[0] for c in curves], [c[1] for c in curves],
                             [c[2] for c in curves], periods=[c[3] for c in curves],

@@ -71,14 +71,14 @@ def assert_same(a, b, name):
 
 def test_static_entry_matches_plan_api_on_two_calls_in_a_row():
     # call 1: astropy-binned geometry, likelihood objective, float32 flux with weights
-    t, y, dy = R.c0_curve(n=15000, seed=11)
+    t, y, dy = R.sector_curve(n=15000, seed=11)
     y32 = y.astype(np.float32)
     w = (1.0 / dy ** 2).astype(np.float32)
-    periods = R.c0_periods(1200)
+    periods = R.sector_periods(1200)
     cfg = SearchConfig("parity", objective="likelihood")
-    rc, msg, got = call_static(t, y32, w, periods, R.C0_DURATIONS, cfg)
+    rc, msg, got = call_static(t, y32, w, periods, R.SECTOR_DURATIONS, cfg)
     assert rc == N.ATB_OK, msg
-    assert_same(got, call_plan(t, y32, w, periods, R.C0_DURATIONS, cfg), "call 1")
+    assert_same(got, call_plan(t, y32, w, periods, R.SECTOR_DURATIONS, cfg), "call 1")
 
     # call 2, straight after: fixed bins, float64 flux, unit weights, unsorted times,
     # a shorter curve -- the array still holds call 1's larger staging
@@ -137,23 +137,23 @@ def test_static_entry_recovers_from_invalid_data_and_runs_without_best_index():
     passes no best-index output, and its grid has more work-queue tiles than
     the launch has CTAs (every CTA takes several tiles)."""
     cfg = SearchConfig("parity", objective="snr")
-    t, y, dy = R.c0_curve(n=4000, seed=12)
+    t, y, dy = R.sector_curve(n=4000, seed=12)
     y32 = y.astype(np.float32)
     w = (1.0 / dy ** 2).astype(np.float32)
     bad = y32.copy()
     bad[1234] = np.nan
-    rc, msg, _ = call_static(t, bad, w, R.c0_periods(300), R.C0_DURATIONS, cfg)
+    rc, msg, _ = call_static(t, bad, w, R.sector_periods(300), R.SECTOR_DURATIONS, cfg)
     assert rc == N.ATB_EDATA and "non-finite" in msg
     # 40 000 periods: 625 tiles of 64 against at most 2 CTAs per SM
     periods = np.geomspace(0.5, 13.7, 40000)
-    rc, msg, got = call_static(t, y32, w, periods, R.C0_DURATIONS, cfg, with_best=False)
+    rc, msg, got = call_static(t, y32, w, periods, R.SECTOR_DURATIONS, cfg, with_best=False)
     assert rc == N.ATB_OK, msg
     assert got["best_index"] == -7  # nothing was written there
-    ref = call_plan(t, y32, w, periods, R.C0_DURATIONS, cfg)
+    ref = call_plan(t, y32, w, periods, R.SECTOR_DURATIONS, cfg)
     got["best_index"] = ref["best_index"]
     assert_same(got, ref, "after invalid data")
     # and a fixed-bin call after it, with the best index, still agrees
     cfg2 = SearchConfig("fast", n_bins=200)
-    rc, msg, got2 = call_static(t, y32, w, R.c0_periods(500), R.C0_DURATIONS, cfg2)
+    rc, msg, got2 = call_static(t, y32, w, R.sector_periods(500), R.SECTOR_DURATIONS, cfg2)
     assert rc == N.ATB_OK, msg
-    assert_same(got2, call_plan(t, y32, w, R.c0_periods(500), R.C0_DURATIONS, cfg2), "fixed")
+    assert_same(got2, call_plan(t, y32, w, R.sector_periods(500), R.SECTOR_DURATIONS, cfg2), "fixed")
