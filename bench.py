@@ -26,6 +26,9 @@ precision` the 512 x 200000-point precision stress.
   cpu_baseline  the CPU restatement of the reference algorithm (FP64, OpenMP
           over every host core) on a bounded sample of the same curves, with
           the engine's errors against it (power, depth, best period, t0)
+  top_k   the device top-5 peaks of every curve (the reference's candidate
+          list) after the timed regions: time per launch, bytes against HBM,
+          and the indices checked against the host rule on a sample of curves
 
 Multi-GPU: `--gpus N` starts N ranks under torchrun (unless already launched
 by torchrun); every rank searches its own share of the curves (weak scaling:
@@ -295,6 +298,52 @@ def cpu_reference(wl, method, budget_s, first=0, max_curves=None):
             break
     dt = time.perf_counter() - t0
     return len(outs) / dt, cores, f"{len(outs)} curves of the workload, all periods", outs, dt
+
+
+def hbm_peak_gbs():
+    """(GB/s, source): the measured copy bandwidth of this pool's B200s when
+    MEASURED_PEAKS.json is present, else the earlier measurement on this pool."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured copy bandwidth (MEASURED_PEAKS.json)"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback: earlier copy-bandwidth measurement on this pool"
+
+
+def top_k_report(plan, stream, host_power, out_begin, counts, k=5, distance=10, launches=5,
+                 sample=64):
+    """Device top-k peaks of every curve (atb_plan_top_k: the reference's
+    get_top_k_candidates(k=5, min_dist_bins=10), gpu_bls.py:146-174) after the
+    timed regions: mean CUDA-event time per launch on the plan's stream, the
+    algorithmic bytes (each curve's power read once, k indices written) against
+    HBM, and the device indices checked against the host rule on `sample`
+    curves."""
+    import torch
+    from astro_transit_gpu_b200.gpu_bls import top_peak_indices
+    got = plan.top_k(k, distance, stream)  # warm-up, and the result checked below
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(launches):
+        plan.top_k(k, distance, stream)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / launches
+    got = got.cpu().numpy()
+    nc = len(counts)
+    ok = all([int(i) for i in got[c] if i >= 0] ==
+             top_peak_indices(host_power[int(out_begin[c]):int(out_begin[c]) + int(counts[c])],
+                              k, distance)
+             for c in range(min(sample, nc)))
+    nbytes = 4.0 * float(np.sum(counts)) + 4.0 * k * nc
+    peak, source = hbm_peak_gbs()
+    achieved = nbytes / (ms * 1e-3) / 1e9
+    return {"kernel": "topk_peaks_kernel", "k": k, "distance": distance, "ms": ms,
+            "launches_timed": launches, "bytes_per_launch": nbytes,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": source},
+            "equals_host_rule_on_curves": min(sample, nc) if ok else 0,
+            "matches_host": bool(ok)}
 
 
 def plain_gpu_baseline(wl, budget_s, device):
@@ -637,6 +686,13 @@ def main(argv=None):
                             lambda c: curve_periods(periods, c)),
             "reference": "oracle FP64 restatement of the reference kernel (fold, sums, windows "
                          "all FP64)"}
+    if rank == 0:
+        try:  # an extra report: a failure here must not lose the measured line
+            line["top_k"] = top_k_report(
+                plan, stream, sess.host_out["power"].numpy(), np.asarray(sess.batch.out_begin),
+                np.array([len(curve_periods(periods, c)) for c in range(nc)], np.int64))
+        except Exception as e:  # noqa: BLE001
+            line["top_k"] = {"error": repr(e)}
     gp = sess.host_out["power"].numpy().copy()  # the resident run's outputs
     gd = sess.host_out["depth"].numpy().copy()
     gt = sess.host_out["t0"].numpy().copy()
