@@ -303,7 +303,7 @@ def cpu_reference(wl, method, budget_s, first=0, max_curves=None):
 def hbm_peak_gbs():
     """(GB/s, source): the measured copy bandwidth of this pool's B200s when
     MEASURED_PEAKS.json is present, else the earlier measurement on this pool."""
-    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
         with open(path) as f:
             return float(json.load(f)["hbm_gbs"]), "measured copy bandwidth (MEASURED_PEAKS.json)"
@@ -653,8 +653,12 @@ def main(argv=None):
             "bound": "smem",
             "kernel": "search_kernel<FIXED>" if args.method == "fast" else "search_kernel<BINNED>",
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": measured_traffic(nc) if args.workload == "uniform" and args.method == "parity"
-            else None,
+            "traffic": measured_traffic(
+                args.workload, args.method, nc,
+                search_algorithmic_bytes(lens, [len(curve_periods(periods, c))
+                                                for c in range(nc)])),
+            "traffic_source": "ncu capture of a smaller launch of this workload under profiles/, "
+                              "scaled to this launch (null: no capture of this workload)",
             "units": "4 B per 32-bit shared-memory reduction the fold issues: 2, 3 or 4 per "
                      "(point, period) update by the curve's histogram layout (tight, count, "
                      f"split; a checked tight period that is folded again counts 2); "
@@ -790,13 +794,30 @@ class ClockSampler:
                 "samples": len(self.rows)}
 
 
-def measured_traffic(n_curves):
-    """DRAM bytes per search launch from the committed ncu capture, scaled to
-    this launch's number of curves (traffic grows in proportion), or None."""
-    path = os.path.join(ROOT, "profiles", "search_kernel_uniform_batch.json")
+def search_algorithmic_bytes(lens, counts):
+    """Bytes one search launch must move: 16 B per staged point (curves start
+    at multiples of 32 points), 8 B per period read and 28 B of outputs per
+    period written."""
+    n_pad = (np.asarray(lens, np.int64) + 31) // 32 * 32
+    return float(16 * n_pad.sum() + 36 * np.asarray(counts, np.int64).sum())
+
+
+def measured_traffic(workload, method, n_curves, algo_bytes):
+    """DRAM bytes per search launch from the committed ncu capture of the same
+    workload and method, scaled to this launch (by curves for the uniform
+    batch, by algorithmic bytes for the uneven one: both captures moved their
+    algorithmic bytes, so traffic grows in proportion), or None."""
+    if workload == "uniform" and method == "parity":
+        name = "search_kernel_uniform_batch.json"
+    elif workload == "mixed" and method == "fast":
+        name = "search_kernel_fixed_uneven_batch.json"
+    else:
+        return None
     try:
-        with open(path) as f:
+        with open(os.path.join(ROOT, "profiles", name)) as f:
             prof = json.load(f)
+        if "capture_algorithmic_bytes" in prof:
+            return prof["dram_bytes_per_launch"] * algo_bytes / prof["capture_algorithmic_bytes"]
         return prof["dram_bytes_per_launch"] * n_curves / prof["capture_curves"]
     except (OSError, KeyError, ValueError):
         return None

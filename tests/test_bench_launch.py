@@ -48,3 +48,28 @@ def test_indexed_uneven_batch_is_split_by_lpt_without_overlap():
     b = R.mixed_curve_indexed(2000, 5)
     assert all(np.array_equal(x, y) for x, y in zip(a, b))
     assert len(a[0]) == specs[5][2] and len(a[3]) == specs[5][3]
+
+
+def test_traffic_is_scaled_from_the_committed_captures():
+    """roofline.traffic: the committed ncu captures give their own launches'
+    DRAM bytes back, and scale with curves (uniform) or algorithmic bytes
+    (uneven)."""
+    import json
+    import os
+    import bench
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    uni = json.load(open(os.path.join(root, "profiles", "search_kernel_uniform_batch.json")))
+    fix = json.load(open(os.path.join(root, "profiles", "search_kernel_fixed_uneven_batch.json")))
+    assert bench.measured_traffic("uniform", "parity", uni["capture_curves"], 1.0) == \
+        uni["dram_bytes_per_launch"]
+    assert bench.measured_traffic("uniform", "parity", 4096, 1.0) == \
+        4 * uni["dram_bytes_per_launch"]
+    a = fix["capture_algorithmic_bytes"]
+    assert bench.measured_traffic("mixed", "fast", 512, a) == fix["dram_bytes_per_launch"]
+    assert bench.measured_traffic("mixed", "fast", 8192, 16 * a) == \
+        16 * fix["dram_bytes_per_launch"]
+    assert bench.measured_traffic("mixed", "parity", 8192, a) is None
+    # the capture's algorithmic bytes are those of its 512 curves
+    import recipes as R
+    cs = [R.mixed_curve_indexed(2000, i) for i in range(512)]
+    assert bench.search_algorithmic_bytes([len(c[0]) for c in cs], [len(c[3]) for c in cs]) == a
