@@ -30,3 +30,25 @@ def test_table_ignores_other_devices_versions_and_bad_files(tmp_path):
         f.write("{not json")
     assert TuningTable(path, "NVIDIA B200", "lib 1").load().entries == {}
     assert TuningTable(str(tmp_path / "missing.json"), "x", "y").load().entries == {}
+
+
+def test_tuned_config_fills_only_knobs_left_at_zero(tmp_path):
+    """BLSEngine.tuned_config takes every knob the config leaves at 0 (tile
+    size, fold threshold, CTA size) from the table entry of the batch's kind,
+    and keeps the ones the caller set; no entry, no change."""
+    from types import SimpleNamespace
+    from astro_transit_gpu_b200.engine import BLSEngine, SearchConfig
+    table = TuningTable(str(tmp_path / "t.json"), "NVIDIA B200", "lib 1")
+    key = ("fast", 11, 14, 15)
+    table.put(key, {"tile_periods": 32, "merge_run": 16, "cta_threads": 256, "best_ms": 1.0})
+    fake = SimpleNamespace(tuning=table, tune_key=lambda batch, config: key)
+    cfg = BLSEngine.tuned_config(fake, None, SearchConfig("fast", n_bins=200))
+    assert (cfg.tile_periods, cfg.merge_run, cfg.cta_threads) == (32, 16, 256)
+    cfg = BLSEngine.tuned_config(fake, None, SearchConfig("fast", tile_periods=8, cta_threads=512))
+    assert (cfg.tile_periods, cfg.merge_run, cfg.cta_threads) == (8, 16, 512)
+    # an entry from before the CTA-size knob existed leaves it at the default
+    table.put(key, {"tile_periods": 16, "merge_run": 0})
+    cfg = BLSEngine.tuned_config(fake, None, SearchConfig("fast"))
+    assert (cfg.tile_periods, cfg.merge_run, cfg.cta_threads) == (16, 0, 0)
+    fake.tune_key = lambda batch, config: ("parity", 1, 1, 1)
+    assert BLSEngine.tuned_config(fake, None, SearchConfig("parity")) == SearchConfig("parity")
