@@ -52,3 +52,31 @@ def test_tuned_config_fills_only_knobs_left_at_zero(tmp_path):
     assert (cfg.tile_periods, cfg.merge_run, cfg.cta_threads) == (16, 0, 0)
     fake.tune_key = lambda batch, config: ("parity", 1, 1, 1)
     assert BLSEngine.tuned_config(fake, None, SearchConfig("parity")) == SearchConfig("parity")
+
+
+def test_autotune_searches_cta_then_tile_then_fold(tmp_path):
+    """BLSEngine.autotune with a stand-in timer: it keeps the fastest CTA
+    size, then the fastest tile at that size, then the fastest fold threshold
+    at both, stores the result for the batch's kind and persists it."""
+    from types import SimpleNamespace
+    from astro_transit_gpu_b200.engine import BLSEngine, SearchConfig
+    cost = {"cta": {512: 10.0, 256: 8.0}, "tile": {8: 3.0, 16: 1.0, 32: 2.0, 64: 2.5},
+            "fold": {0: 0.5, -1: 0.9, 4: 0.2, 16: 0.7}}
+    seen = []
+
+    def timer(batch, cfg, repeats):
+        seen.append((cfg.cta_threads, cfg.tile_periods, cfg.merge_run))
+        return (cost["cta"][cfg.cta_threads] + cost["tile"].get(cfg.tile_periods, 0.0)
+                + cost["fold"][cfg.merge_run])
+
+    table = TuningTable(str(tmp_path / "t.json"), "NVIDIA B200", "lib 1")
+    key = ("fast", 11, 14, 15)
+    fake = SimpleNamespace(tuning=table, tune_key=lambda batch, config: key, _time_search=timer)
+    best = BLSEngine.autotune(fake, None, SearchConfig("fast"))
+    assert best == {"cta_threads": 256, "tile_periods": 16, "merge_run": 4}
+    # the CTA sizes first (tile and fold at the config's), then tiles, then folds
+    assert seen[:2] == [(512, 0, 0), (256, 0, 0)]
+    assert seen[2:6] == [(256, tp, 0) for tp in (8, 16, 32, 64)]
+    assert seen[6:] == [(256, 16, mr) for mr in (0, -1, 4, 16)]
+    again = TuningTable(table.path, "NVIDIA B200", "lib 1").load().get(key)
+    assert {k: again[k] for k in best} == best
