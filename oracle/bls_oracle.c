@@ -355,6 +355,15 @@ int orc_ref_fixed(int64_t n, const double* t, const double* y, const double* w, 
 /* (B) the engine's exact arithmetic                                          */
 /* ------------------------------------------------------------------------- */
 
+/* A window length in bins from its real value, as the engine forms it: at
+ * least 1 (NaN: 1) and at most 2^28 (every bin count is below 2^27, so a
+ * clamped window is skipped exactly as the unclamped one). */
+static int eng_len(double v)
+{
+    if (v >= 268435456.0) return 268435456;
+    return v >= 1.0 ? (int)v : 1;
+}
+
 /* Per-point fixed-point magnitude bound |q| <= 2^qbits with
  * qbits = min(27, 63 - 2*bitlen(n)), bitlen(n) = number of bits of the point
  * count n: the engine's 32-bit split histogram words cannot overflow. */
@@ -599,7 +608,7 @@ int orc_eng_binned(int64_t n, const double* dt, const int32_t* qw, const int32_t
     const double inv_bin_dur = 1.0 / bin_dur;
     int dur_bins[64];
     if (nd > 64) return ORC_EINVAL;
-    for (int k = 0; k < nd; ++k) dur_bins[k] = (int)round(durations[k] * inv_bin_dur);
+    for (int k = 0; k < nd; ++k) dur_bins[k] = eng_len(round(durations[k] * inv_bin_dur));
     double pmax = periods[0];
     for (int64_t p = 1; p < np; ++p)
         if (periods[p] > pmax) pmax = periods[p];
@@ -766,8 +775,7 @@ int orc_eng_fixed(int64_t n, const double* dt, const int32_t* qw, const int32_t*
                     kc.thr = 0.0;
                     for (int s = 0; s < n_bins; ++s) {
                         for (int k = 0; k < nd; ++k) {
-                            int L = (int)fma(durations[k] * inv_p, nbd, 0.5);
-                            if (L < 1) L = 1;
+                            const int L = eng_len(fma(durations[k] * inv_p, nbd, 0.5));
                             if (L >= n_bins) continue;
                             double dw, dy;
                             float fdw;
@@ -795,8 +803,7 @@ int orc_eng_fixed(int64_t n, const double* dt, const int32_t* qw, const int32_t*
                     t0[p] = 0.0; duration[p] = 0.0f; window[p] = -1;
                 } else {
                     const int s = best.key / nd, k = best.key % nd;
-                    int L = (int)fma(durations[k] * inv_p, nbd, 0.5);
-                    if (L < 1) L = 1;
+                    const int L = eng_len(fma(durations[k] * inv_p, nbd, 0.5));
                     double dw, dy;
                     if (s + L <= n_bins) {
                         dw = cw[s + L] - cw[s];
