@@ -3089,14 +3089,16 @@ extern "C" int atb_search_curve_static(const atb_params* prm, const double* t, c
     int* sqy = reinterpret_cast<int*>(base + kOffQy);
     StaticMeta* m = reinterpret_cast<StaticMeta*>(base + kOffMeta);
 
-    const long long n_tiles = (n_periods + kTileP - 1) / kTileP;
-    static_meta_init<<<1, 32, 0, s>>>(m, n, n_periods, n_durations, n_tiles);
-
     // fixed bins: one histogram of n_bins per period must fit shared memory
+    // (checked before the first launch, so that a rejected call leaves no work
+    // in flight on the shared array)
     if (prm->geometry == ATB_GEOM_FIXED && prm->n_bins + 2 > cap)
         return static_fail(err, err_len, ATB_EINVAL,
                            "n_bins=%d; this entry point holds at most %d bins per period "
                            "(use the plan API)", prm->n_bins, cap - 2);
+    const long long n_tiles = (n_periods + kTileP - 1) / kTileP;
+    static_meta_init<<<1, 32, 0, s>>>(m, n, n_periods, n_durations, n_tiles);
+
     if (prm->geometry == ATB_GEOM_BINNED)
         nbins_max_kernel<<<1, 256, 0, s>>>(1, m->per_beg, m->per_cnt, m->dur_beg, m->dur_cnt,
                                            periods, durations, prm->oversample, prm->max_bins,
