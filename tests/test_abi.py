@@ -4,8 +4,6 @@ import ctypes
 import os
 import re
 
-import pytest
-
 from astro_transit_gpu_b200 import _native as N
 from astro_transit_gpu_b200 import build as B
 
