@@ -261,3 +261,24 @@ def test_oracle_rejects_bad_arguments():
         O.ref_fixed(t, t, None, [1.0], [0.1], n_bins=1)
     with pytest.raises(ValueError):
         O.eng_stage(t, t, np.zeros(10, np.float32))
+
+
+@pytest.mark.parametrize("geometry", ["binned", "fixed"])
+def test_engine_mirror_windows_longer_than_any_period_are_skipped(geometry):
+    """A duration whose window is longer than every period's bin count (here
+    1e12 d, far beyond 2^31 bins, where the engine clamps window lengths to
+    2^28 bins) never wins: the outputs equal the search without it, with the
+    same window keys since it is the last duration."""
+    t, y, dy = R.sector_curve(n=3000, seed=5)
+    w = (1.0 / dy ** 2).astype(np.float32)
+    periods = R.sector_periods(200)
+    durs = [0.05, 0.1]
+    run = (lambda d: O.eng_binned(t, y.astype(np.float32), w, periods, d, objective="snr")) \
+        if geometry == "binned" else \
+        (lambda d: O.eng_fixed(t, y.astype(np.float32), w, periods, d, n_bins=200))
+    a, b = run(durs), run(durs + [1e12])
+    for k in ("power", "depth", "depth_err", "t0", "duration"):
+        assert np.array_equal(a[k], b[k]), k
+    # window keys are start * n_durations + duration index
+    ok = a["window"] >= 0
+    assert np.array_equal(a["window"][ok] // 2 * 3 + a["window"][ok] % 2, b["window"][ok])
