@@ -104,6 +104,24 @@ def prune(pending, now: float):
     return keep, expired, cancelled
 
 
+def check_request(t: np.ndarray, y: np.ndarray, dy, periods: np.ndarray,
+                  durations: np.ndarray) -> None:
+    """Reject, at submission, what would fail a whole batch later: one
+    request's invalid data makes the engine report ATB_EDATA for the batch it
+    joins, so every other request in that batch would fail with it.  The rules
+    are the reference's (search/api.py:53-70) plus the engine's grid limits."""
+    if len(t) < 1:
+        raise ValueError("a request needs at least one point")
+    if not (np.all(np.isfinite(t)) and np.all(np.isfinite(y))):
+        raise ValueError("Input time or flux contains NaNs or infinite values.")
+    if dy is not None and not np.all(np.isfinite(dy) & (dy > 0)):
+        raise ValueError("flux_err must be finite and strictly positive.")
+    if len(periods) < 1 or not np.all(np.isfinite(periods) & (periods > 0)):
+        raise ValueError("periods must be positive and finite")
+    if not 1 <= len(durations) <= 32 or not np.all(np.isfinite(durations) & (durations > 0)):
+        raise ValueError("durations: 1 to 32, positive and finite")
+
+
 def request_bytes(n_points: int, n_periods: int, n_durations: int) -> int:
     """Device bytes a request holds while its batch runs: inputs (t f64, y, w
     f32), staged points (16 B), the grids and the per-period outputs (28 B),
@@ -175,6 +193,7 @@ class BLSServer:
         cfg.params()  # validates the combination
         per = np.atleast_1d(np.asarray(periods, np.float64))
         dur = np.atleast_1d(np.asarray(durations, np.float64))
+        check_request(t, y, dy, per, dur)
         now = time.perf_counter()
         req = _Request(t, y, w, per, dur, cfg, fdt,
                        request_bytes(len(t), len(per), len(dur)), now,

@@ -56,3 +56,33 @@ def test_prune_drops_expired_and_cancelled_requests_in_order():
     assert names(keep) == ["a", "d"] and names(expired) == ["b"] and names(cancelled) == ["c"]
     keep, expired, cancelled = prune([a, b, d], now=1.0)
     assert names(keep) == ["a", "b", "d"] and not expired and not cancelled
+
+
+def test_requests_that_would_fail_a_batch_are_rejected_at_submission():
+    """A request with invalid data would make the whole batch it joins fail
+    (the engine flags the batch), so submit() rejects it on its own."""
+    import numpy as np
+    import pytest
+    from astro_transit_gpu_b200.serving import check_request
+    t = np.linspace(0.0, 27.0, 500)
+    y = np.ones(500, np.float32)
+    dy = np.full(500, 1e-3)
+    per, dur = np.array([1.0, 2.0]), np.array([0.05, 0.1])
+    check_request(t, y, dy, per, dur)  # valid
+    check_request(t, y, None, per, dur)
+    bad_y = y.copy()
+    bad_y[7] = np.nan
+    bad_dy = dy.copy()
+    bad_dy[3] = 0.0
+    cases = [
+        ((t[:0], y[:0], None, per, dur), "at least one point"),
+        ((t, bad_y, dy, per, dur), "NaNs"),
+        ((t, y, bad_dy, per, dur), "flux_err"),
+        ((t, y, dy, np.array([1.0, -1.0]), dur), "periods"),
+        ((t, y, dy, np.array([]), dur), "periods"),
+        ((t, y, dy, per, np.array([0.05, np.inf])), "durations"),
+        ((t, y, dy, per, np.linspace(0.01, 0.3, 33)), "durations"),
+    ]
+    for args, msg in cases:
+        with pytest.raises(ValueError, match=msg):
+            check_request(*args)
