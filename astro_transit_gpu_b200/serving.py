@@ -116,6 +116,8 @@ def check_request(t: np.ndarray, y: np.ndarray, dy, periods: np.ndarray,
         raise ValueError("Input time or flux contains NaNs or infinite values.")
     if dy is not None and not np.all(np.isfinite(dy) & (dy > 0)):
         raise ValueError("flux_err must be finite and strictly positive.")
+    if dy is not None and not np.all(np.isfinite((1.0 / (dy * dy)).astype(np.float32))):
+        raise ValueError("flux_err too small: its float32 weight 1/flux_err^2 overflows")
     if len(periods) < 1 or not np.all(np.isfinite(periods) & (periods > 0)):
         raise ValueError("periods must be positive and finite")
     if not 1 <= len(durations) <= 32 or not np.all(np.isfinite(durations) & (durations > 0)):

@@ -78,6 +78,7 @@ def test_requests_that_would_fail_a_batch_are_rejected_at_submission():
         ((t[:0], y[:0], None, per, dur), "at least one point"),
         ((t, bad_y, dy, per, dur), "NaNs"),
         ((t, y, bad_dy, per, dur), "flux_err"),
+        ((t, y, np.full(500, 1e-25), per, dur), "overflows"),
         ((t, y, dy, np.array([1.0, -1.0]), dur), "periods"),
         ((t, y, dy, np.array([]), dur), "periods"),
         ((t, y, dy, per, np.array([0.05, np.inf])), "durations"),
