@@ -116,8 +116,11 @@ def check_request(t: np.ndarray, y: np.ndarray, dy, periods: np.ndarray,
         raise ValueError("Input time or flux contains NaNs or infinite values.")
     if dy is not None and not np.all(np.isfinite(dy) & (dy > 0)):
         raise ValueError("flux_err must be finite and strictly positive.")
-    if dy is not None and not np.all(np.isfinite((1.0 / (dy * dy)).astype(np.float32))):
-        raise ValueError("flux_err too small: its float32 weight 1/flux_err^2 overflows")
+    if dy is not None:
+        with np.errstate(over="ignore"):
+            w = (1.0 / (dy * dy)).astype(np.float32)
+        if not np.all(np.isfinite(w)):
+            raise ValueError("flux_err too small: its float32 weight 1/flux_err^2 overflows")
     if len(periods) < 1 or not np.all(np.isfinite(periods) & (periods > 0)):
         raise ValueError("periods must be positive and finite")
     if not 1 <= len(durations) <= 32 or not np.all(np.isfinite(durations) & (durations > 0)):
@@ -188,7 +191,8 @@ class BLSServer:
             dy = np.asarray(dy, np.float64)
             if len(dy) != len(y):
                 raise ValueError("flux_err and flux must have the same length")
-            w = (1.0 / (dy * dy)).astype(np.float32)
+            with np.errstate(over="ignore"):  # an overflow is rejected below
+                w = (1.0 / (dy * dy)).astype(np.float32)
         cfg = (SearchConfig("fast", n_bins=int(n_bins)) if method == "fast" else
                SearchConfig("parity", objective=objective or "snr", oversample=int(oversample),
                             max_bins=max_bins))
