@@ -191,7 +191,7 @@ class BLSServer:
             dy = np.asarray(dy, np.float64)
             if len(dy) != len(y):
                 raise ValueError("flux_err and flux must have the same length")
-            with np.errstate(over="ignore"):  # an overflow is rejected below
+            with np.errstate(over="ignore", divide="ignore"):  # rejected below
                 w = (1.0 / (dy * dy)).astype(np.float32)
         cfg = (SearchConfig("fast", n_bins=int(n_bins)) if method == "fast" else
                SearchConfig("parity", objective=objective or "snr", oversample=int(oversample),
